@@ -1,0 +1,225 @@
+/*
+ * cqg.h — C ABI of the B200 Monte Carlo wave-function (MCWF) ensemble engine.
+ *
+ * The engine replaces C++QED's EnsembleMCWF / MCWF_Trajectory hot path.  The
+ * reference evaluates its quantum system through virtual callbacks
+ * (structure::Hamiltonian::addContribution, Liouvillean::rates / actWithJ,
+ * Averaged::average, Exact::actWithU) that cannot run on a GPU, so the system
+ * is lowered ONCE on the host into the plain descriptor below (banded
+ * "Tridiagonal" terms placed on tensor-product axes, jump operators with their
+ * closed-form rates, linear observables) and every trajectory step then runs
+ * on the device.
+ *
+ * Conventions
+ *  - Complex numbers are two doubles {re, im}; layout-compatible with
+ *    std::complex<double> and double2.
+ *  - State vectors are C-order (last axis contiguous), as Blitz CArray<RANK>
+ *    in the reference (quantumdata/Types.h:11-12).
+ *  - Every function returns 0 on success or a negative CQG_E_* code; the
+ *    message is available from cqg_last_error() (thread-local).
+ *  - Handles are not thread-safe; distinct handles are independent.
+ */
+#ifndef CQG_H_INCLUDED
+#define CQG_H_INCLUDED
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CQG_MAX_RANK 8
+#define CQG_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define CQG_OK 0
+#define CQG_E_INVALID (-1)       /* bad argument / inconsistent descriptor       */
+#define CQG_E_CUDA (-2)          /* CUDA runtime error                            */
+#define CQG_E_NOMEM (-3)         /* allocation failed / HBM budget exceeded       */
+#define CQG_E_UNSUPPORTED (-4)   /* descriptor outside what the kernels handle   */
+#define CQG_E_NONFINITE (-5)     /* a trajectory produced a non-finite value      */
+#define CQG_E_STALLED (-6)       /* a trajectory exhausted its attempt budget     */
+#define CQG_E_NODEVICE (-7)      /* no CUDA device / extension not usable         */
+
+/* per-trajectory status bits (cqg_ensemble_status) */
+#define CQG_TRAJ_NONFINITE_NORM 1u   /* MCWF_Trajectory.h:338 "Infinite detected"   */
+#define CQG_TRAJ_NONFINITE_RATE 2u   /* LiouvilleanAveragedCommon.h:87-89           */
+#define CQG_TRAJ_DT_UNDERFLOW 4u     /* step size collapsed below 1e-300 * t scale  */
+#define CQG_TRAJ_ATTEMPT_LIMIT 8u    /* bounded retry loop gave up                  */
+
+typedef struct cqg_complex {
+  double re, im;
+} cqg_complex;
+
+/* ---- system descriptor ---------------------------------------------------
+ * A banded operator in the sense of quantumoperator::Tridiagonal<RANK>
+ * (quantumoperator/Tridiagonal.h:71-287) placed on `rank` axes of the system.
+ * diagonal index  j = sum_a digit_a * 3^(rank-1-a)   (axis 0 most significant)
+ *   digit 0: main diagonal      out n   <- in n      extent N_a
+ *   digit 1: "minus" diagonal   out n+K <- in n      extent N_a-K_a
+ *   digit 2: "plus"  diagonal   out n   <- in n+K    extent N_a-K_a
+ * (Tridiagonal.tcc:220-263, ranges filled at :199-210).  Each diagonal is
+ * NULL (empty) or a C-order array over its box.  `freqs` (NULL, or 3^rank
+ * entries each NULL or box-shaped) gives the interaction-picture frequencies:
+ * at picture time tau the coefficient is diagonal * exp(tau * freq)
+ * (Tridiagonal::propagate, Tridiagonal.tcc:153-163).                       */
+typedef struct cqg_tridiagonal {
+  int32_t rank;
+  int32_t axes[CQG_MAX_RANK];
+  int64_t differences[CQG_MAX_RANK];
+  const cqg_complex* const* diagonals;
+  const cqg_complex* const* freqs;
+} cqg_tridiagonal;
+
+/* A jump operator J_m (structure::Liouvillean<RANK>::actWithJ, Liouvillean.h:54-60)
+ * with its rate rule.  If rate_weights != NULL the rate is the closed form
+ * sum_n rate_weights[n_axis] |psi_n|^2 over the normalised state (the
+ * reference's element `rate` functions, e.g. 2 kappa <n>, Mode_.h:180-184);
+ * otherwise the rate is ||J psi||^2 and the jump uses the normalised J psi
+ * (the "special jump" convention, MCWF_Trajectory.h:279-291).             */
+typedef struct cqg_jump {
+  cqg_tridiagonal op;
+  int32_t rate_axis;
+  const double* rate_weights;
+} cqg_jump;
+
+/* An observable column source: Re or Im of <psi|O|psi> (linear in rho, as
+ * structure::Averaged::average_v).  O is either a banded term (`dense` NULL)
+ * or a dense N_axis x N_axis row-major matrix acting on `dense_axis`.     */
+typedef struct cqg_observable {
+  cqg_tridiagonal op;
+  const cqg_complex* dense;
+  int32_t dense_axis;
+  int32_t col_re; /* output column of Re<O>, or -1 */
+  int32_t col_im; /* output column of Im<O>, or -1 */
+} cqg_observable;
+
+/* The whole system: Hamiltonian terms H/i in the reference's application
+ * order (frees in axis order, then interactions: BinarySystem.cc:194-207,
+ * Composite.tcc:178-197), the Exact (interaction-picture) part as per-axis
+ * exponents lambda_a[n] with U(tau) = prod_a exp(lambda_a[n_a] tau)
+ * (FreeExact.h:31, Mode.cc:42-45), jumps in the reference's ordinal order,
+ * and observables.                                                          */
+typedef struct cqg_system_desc {
+  int32_t rank;
+  int64_t dims[CQG_MAX_RANK];
+  int32_t n_ham;
+  const cqg_tridiagonal* ham;
+  int32_t has_hamiltonian;                    /* getHa() != nullptr            */
+  const cqg_complex* exact[CQG_MAX_RANK];     /* NULL: axis has no Exact part  */
+  int32_t n_jumps;
+  const cqg_jump* jumps;
+  int32_t n_obs;
+  const cqg_observable* obs;
+  int32_t n_avr;                              /* number of linear average columns */
+  double highest_frequency;                   /* QuantumSystem::highestFrequency */
+} cqg_system_desc;
+
+/* ---- engine parameters (mcwf::Pars, ode_engine::Pars, randomutils::Pars) */
+#define CQG_RNG_PCG64 0   /* pcg64{seed, prngStream+i}: MCWF_Trajectory.h:208,223-226 */
+#define CQG_RNG_PHILOX 1  /* Philox4x32-10 keyed by seed, counter = (traj, draw)     */
+
+#define CQG_FP64 0        /* complex128 state and operator                           */
+#define CQG_FP32 1        /* complex64 state/operator; FP64 norm, error norm, dt, sums */
+
+typedef struct cqg_mcwf_pars {
+  double eps_rel;              /* --eps      (ODE.h:59) default 1e-6  */
+  double eps_abs;              /* --epsAbs   (ODE.h:60) default 1e-12 */
+  double dp_limit;             /* --dpLimit  (MCWF_Trajectory.h:41) 0.01 */
+  double overshoot_tolerance;  /* --overshootTolerance (:42) 10 */
+  double dt_init;              /* <= 0: 1/(10*highest_frequency) (Trajectory.h:126) */
+  uint64_t seed;               /* --seed (Random.h:144) 1001 */
+  uint64_t prng_stream;        /* --prngStream (Random.h:145) 1; trajectory i uses stream+i */
+  int32_t rng;                 /* CQG_RNG_* */
+  int32_t noise;               /* --noise: 0 switches the Liouvillean off (Structure.h:97-103) */
+  int32_t precision;           /* CQG_FP64 / CQG_FP32 */
+  int32_t max_attempts;        /* bounded ODE retries per step (0: default 100000) */
+} cqg_mcwf_pars;
+
+void cqg_mcwf_pars_default(cqg_mcwf_pars* p);
+
+/* ---- errors / device --------------------------------------------------- */
+const char* cqg_last_error(void);
+int cqg_abi_version(void);
+int cqg_device_count(int* count);
+
+/* ---- systems ------------------------------------------------------------
+ * Lower a descriptor to device memory.  Replaces the virtual plugin
+ * interfaces structure::Hamiltonian/Liouvillean/Averaged/Exact
+ * (Hamiltonian.h:38-43, Liouvillean.h:54-67, Averaged.h:37-49, Exact.h:58-61)
+ * and quantumoperator::Tridiagonal::apply (Tridiagonal.tcc:220-233).      */
+typedef struct cqg_system cqg_system;
+int cqg_system_create(const cqg_system_desc* desc, cqg_system** out);
+int cqg_system_dimension(const cqg_system* sys, int64_t* total_dim);
+int cqg_system_destroy(cqg_system* sys);
+
+/* ---- ensembles ----------------------------------------------------------
+ * mcwf::makeEnsemble (MCWF_Trajectory.h:213-234): n_traj copies of psi0
+ * (sys dimension D complex values), trajectory i seeded with stream
+ * prng_stream+i.  Trajectories may belong to different systems
+ * (cqg_batch_create) — the uneven-batch case.                             */
+typedef struct cqg_ensemble cqg_ensemble;
+int cqg_ensemble_create(const cqg_system* sys, const cqg_complex* psi0, int64_t n_traj,
+                        const cqg_mcwf_pars* pars, cqg_ensemble** out);
+
+/* Batch of trajectories over several systems: trajectory i evolves
+ * systems[sys_index[i]] from psi0s + psi0_offsets[i] (host pointer). */
+int cqg_batch_create(const cqg_system* const* systems, int32_t n_systems, const int32_t* sys_index,
+                     const cqg_complex* psi0s, const int64_t* psi0_offsets, int64_t n_traj,
+                     const cqg_mcwf_pars* pars, cqg_ensemble** out);
+
+/* Advance every trajectory by exactly Dt, n_intervals times (cppqedutils::advance,
+ * Trajectory.h:44-50, inside Ensemble::advance, StochasticTrajectory.h:220).
+ * After interval k the ensemble-summed linear averages are written to
+ * avr_out[k*n_avr + c] (host pointer, may be NULL) — divide by n_traj for the
+ * ensemble mean; the reference streams (1/N) Tr(rho O), MCWF_Trajectory.h:406-420.
+ * In batch mode each trajectory's own averages are kept per system; use
+ * cqg_ensemble_traj_averages for them.                                     */
+int cqg_ensemble_run(cqg_ensemble* ens, double Dt, int32_t n_intervals, double* avr_out);
+
+/* Same as cqg_ensemble_run but every trajectory advances to the absolute
+ * time t_end (used for the T-capped final interval in Dt mode). */
+int cqg_ensemble_advance_to(cqg_ensemble* ens, double t_end, double* avr_out);
+
+/* Single trajectory: `n_steps` MCWF steps, each MCWF_Trajectory::step(T - t)
+ * (the dc-mode loop of trajectory::run, Trajectory.h:560-595), stopping early
+ * at T.  Applies to every trajectory of the ensemble. */
+int cqg_ensemble_steps(cqg_ensemble* ens, int32_t n_steps, double T, double* avr_out);
+
+/* Per-trajectory linear averages at the current time: out[i*n_avr + c]. */
+int cqg_ensemble_traj_averages(cqg_ensemble* ens, double* out);
+
+int cqg_ensemble_size(const cqg_ensemble* ens, int64_t* n_traj, int32_t* n_avr);
+int cqg_ensemble_get_state(const cqg_ensemble* ens, int64_t i, cqg_complex* psi_out);
+int cqg_ensemble_set_state(cqg_ensemble* ens, int64_t i, const cqg_complex* psi);
+
+/* Scalars per trajectory (any pointer may be NULL): t, dtDid, dtTry. */
+int cqg_ensemble_get_times(const cqg_ensemble* ens, double* t, double* dt_did, double* dt_try);
+
+/* Logger counters per trajectory (MCWF_TrajectoryLogger.h:59-101, ODE.h:99-122):
+ * counters[i*8 + k], k = 0 accepted steps, 1 ODE attempts, 2 failed ODE attempts,
+ * 3 RHS evaluations, 4 dpLimit overshoots, 5 step-backs, 6 jumps, 7 status bits. */
+int cqg_ensemble_get_counters(const cqg_ensemble* ens, uint64_t* counters);
+
+/* Max overshoot (MCWF logger) and max |norm-1| per trajectory. */
+int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_norm_dev);
+
+/* Jump record ring per trajectory: up to `cap` (time, lindblad) pairs of the
+ * most recent jumps (MCWF logger jump list, MCWF_TrajectoryLogger.cc:42-75). */
+int cqg_ensemble_get_jumps(const cqg_ensemble* ens, int64_t i, int32_t cap, double* times,
+                           int32_t* lindblads, int32_t* n_out);
+
+/* OR of all trajectory status bits; CQG_E_NONFINITE / CQG_E_STALLED when set. */
+int cqg_ensemble_status(const cqg_ensemble* ens, uint32_t* bits);
+
+/* Device time of the last run call in milliseconds (CUDA events). */
+int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* ms);
+
+int cqg_ensemble_destroy(cqg_ensemble* ens);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CQG_H_INCLUDED */
