@@ -1,0 +1,318 @@
+"""Benchmark of the MCWF ensemble engine (one JSON line on rank 0).
+
+Workload (default): the driven lossy qubit-mode system — two-level atom x mode with
+Jaynes-Cummings coupling g=2, kappa=1, gamma=0.5, pump eta=1.5, Delta=0, dimension
+2 x 40 = 80, complex128, 4096 trajectories per GPU, RK54 eps=1e-6, dpLimit 0.01 —
+evolved through t in [0, 20].  One bench "step" advances every trajectory by Dt=1
+(inside the same persistent launch the trajectories take ~10^3 MCWF steps each).
+The metric is accepted MCWF trajectory-steps per second (MCWF_Trajectory::step calls,
+logger_.step(), MCWF_Trajectory.h:372) summed over all GPUs.
+
+--impl reference times the reference's algorithm on the host cores (the CPU oracle,
+a restatement of C++QED's serial Ensemble / MCWF_Trajectory path including the
+density-operator average at every Dt) on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): trajectories are sharded, every rank runs its own 4096 with
+disjoint pcg/philox streams (weak scaling); the per-interval ensemble sums are
+all-reduced (the only exchange) and timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (script, args, n_traj per GPU, Dt per step)
+    "qbitmode_jc_2x40": ("QbitMode_C++QED",
+                         ["--picture", "Sch", "--deltaA", "0", "--gamma", "0.5", "--deltaC", "0", "--kappa", "1",
+                          "--eta", "1.5", "--cutoff", "40", "--g", "2"], 4096, 1.0),
+    "pumped_lossy_mode_30": ("PumpedLossyMode_C++QED",
+                             ["--picture", "Sch", "--deltaC", "-1", "--eta", "2", "--kappa", "1", "--cutoff", "30",
+                              "--no_quadratures"], 1000, 1.0),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="qbitmode_jc_2x40", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
+    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sms.append(float(p[1]))
+                maxes.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def flops_model(model):
+    """Algorithmic FLOPs per RK attempt and per extra MCWF-step work, from the system's
+    operator structure (complex MAC = 8, complex multiply = 6, real-complex axpy = 4)."""
+    import numpy as np
+    d = model.desc.contents
+    D = model.dim
+    # nonzeros of H/i per row: count entries of every term
+    nnz = 0
+    for i in range(d.n_ham):
+        t = d.ham[i]
+        L = 3 ** t.rank
+        for j in range(L):
+            if t.diagonals[j]:
+                box = 1
+                digits = []
+                rem = j
+                for _ in range(t.rank):
+                    digits.append(rem % 3)
+                    rem //= 3
+                digits = digits[::-1]
+                for a in range(t.rank):
+                    N = d.dims[t.axes[a]]
+                    box *= N if digits[a] == 0 else N - t.differences[a]
+                slices = D // int(np.prod([d.dims[t.axes[a]] for a in range(t.rank)]))
+                nnz += box * slices
+    rhs = 8.0 * nnz
+    per_attempt = 6 * rhs + D * (15 * 4 + 4 * 4 + 5 * 4 + 15)
+    per_step = D * (5 + 3 * d.n_jumps)
+    return per_attempt, per_step, nnz
+
+
+def run_ours(args, rank, world, dev):
+    import numpy as np
+    import torch
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+    model = cqg.Model(script, sargs)
+    pars = model.run_pars().mcwf
+    pars.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
+    pars.precision = A.FP64 if args.precision == "fp64" else A.FP32
+    pars.prng_stream = 1 + rank * n_traj
+    system = cqg.System(model.desc)
+    psi0 = model.initial_state()
+    ens = cqg.Ensemble(system, psi0, n_traj, pars)
+
+    def allreduce(x):
+        if world > 1:
+            t = torch.tensor(x, dtype=torch.float64, device="cuda")
+            torch.distributed.all_reduce(t)
+            return t.cpu().numpy()
+        return x
+
+    for _ in range(args.warmup):
+        allreduce(ens.run(Dt, 1))
+    c0 = ens.counters()
+    sampler = ClockSampler(dev)
+    if rank == 0:
+        sampler.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    kernel_ms = run_ms = 0.0
+    for _ in range(args.steps):
+        sums = allreduce(ens.run(Dt, 1))
+        k, r = ens.last_ms()
+        kernel_ms += k
+        run_ms += r
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = sampler.stop() if rank == 0 else None
+    c1 = ens.counters()
+    d = (c1.astype(np.int64) - c0.astype(np.int64)).sum(axis=0)
+    steps_local, attempts_local, rhs_local = int(d[0]), int(d[1]), int(d[3])
+    tot = allreduce(np.array([steps_local, attempts_local, rhs_local], dtype=np.float64))
+    tmax = allreduce(np.array([run_ms, kernel_ms])) if world == 1 else None
+    if world > 1:
+        t = torch.tensor([run_ms, kernel_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tmax = t.cpu().numpy()
+    run_ms_max, kernel_ms_max = float(tmax[0]), float(tmax[1])
+    steps_total = float(tot[0])
+    value = steps_total / (run_ms_max * 1e-3)
+
+    # end to end through the public API from host buffers: create (upload of the host
+    # states), one Dt interval, read-back of the averages, destroy
+    e2e_steps = 0
+    t0 = time.perf_counter()
+    n_e2e = max(1, min(3, args.steps))
+    for _ in range(n_e2e):
+        e = cqg.Ensemble(system, psi0, n_traj, pars)
+        allreduce(e.run(Dt, 1))
+        e2e_steps += int(e.counters()[:, 0].sum())
+        del e
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_tot = allreduce(np.array([e2e_steps, e2e_s], dtype=np.float64))
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = float(e2e_tot[0]) / e2e_s
+    h2d = n_traj * model.dim * 16 + n_traj * (8 * 4 + 32 + 64)
+    d2h = (model.n_avr + 1) * 8 + 4
+
+    fp64_peak, fp32_peak = cqg.engine.probe_fma_peaks()
+    per_attempt, per_step, nnz = flops_model(model)
+    flops = float(tot[1]) * per_attempt + steps_total * per_step
+    achieved = flops / (kernel_ms_max * 1e-3) / 1e12
+    peak = fp64_peak if args.precision == "fp64" else fp32_peak
+    return {
+        "value": value, "ms_per_step": run_ms_max / args.steps, "steps_total": steps_total,
+        "attempts_total": float(tot[1]), "rhs_total": float(tot[2]), "kernel_ms": kernel_ms_max,
+        "clocks": clocks, "e2e": {"value": e2e_value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": h2d,
+                                  "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU",
+                     "flops_per_attempt": per_attempt, "nnz_h": nnz},
+        "n_traj": n_traj, "model": model,
+    }
+
+
+def cpu_sample(args, threads, seconds):
+    """Times the oracle (the reference's serial algorithm) on a bounded sample."""
+    import cppqed_b200 as cqg
+    from tests.oracle_lib import Oracle
+
+    script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+    model = cqg.Model(script, sargs)
+    pars = model.run_pars().mcwf
+    orc = Oracle()
+    # calibrate: a few trajectories over one Dt
+    n = max(threads, 4)
+    steps, secs, _ = orc.ensemble_bench(model, pars, n, Dt, 1, threads, 1)
+    per_traj = secs / n
+    n = max(threads, int(seconds / max(per_traj, 1e-6)))
+    n = min(n, n_traj)
+    steps, secs, _ = orc.ensemble_bench(model, pars, n, Dt, 1, threads, 1)
+    return {"value": steps / secs, "unit": "trajectory-steps/s", "cores": threads, "kind": "port",
+            "sample": "%d trajectories x Dt=%g of %s (of %d), serial Ensemble::advance + rho average per Dt" %
+                      (n, Dt, args.workload, n_traj), "steps": steps, "seconds": secs}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and "RANK" in os.environ:
+        world = int(os.environ["WORLD_SIZE"])
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        res = []
+        for _ in range(args.warmup):
+            pass
+        for _ in range(args.steps):
+            res.append(cpu_sample(args, threads, max(1.0, args.cpu_sample_seconds / max(args.steps, 1))))
+        value = sum(r["steps"] for r in res) / sum(r["seconds"] for r in res)
+        script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+        out = {"metric": "MCWF trajectory-steps/s", "value": value, "unit": "trajectory-steps/s",
+               "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": 1e3 * sum(r["seconds"] for r in res) / len(res), "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": args.workload, "script": script, "args": " ".join(sargs),
+                          "n_traj_per_gpu": n_traj, "Dt_per_step": Dt},
+               "impl": "reference",
+               "cpu_baseline": {"value": value, "unit": "trajectory-steps/s", "cores": threads, "kind": "port",
+                                "sample": res[0]["sample"]},
+               "e2e": {"value": value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = run_ours(args, rank, world, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(args, 1, args.cpu_sample_seconds)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+        out = {"metric": "MCWF trajectory-steps/s", "value": r["value"], "unit": "trajectory-steps/s",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
+               "config": {"workload": args.workload, "script": script, "args": " ".join(sargs),
+                          "n_traj_per_gpu": n_traj, "Dt_per_step": Dt, "rng": args.rng,
+                          "l2_flush": "not needed: states stay on chip; per-step HBM traffic is the state read/write",
+                          "parallelism": "trajectory-sharded x%d" % world},
+               "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"],
+               "gpu_launches": 3 * args.steps,
+               "counters": {"accepted_steps": r["steps_total"], "ode_attempts": r["attempts_total"],
+                            "rhs_evaluations": r["rhs_total"], "kernel_ms": r["kernel_ms"]}}
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

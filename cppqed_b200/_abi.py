@@ -135,7 +135,8 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_get_jumps": (C.c_int, [_P, C.c_int64, C.c_int32, _DP, C.POINTER(C.c_int32),
                                          C.POINTER(C.c_int32)]),
     "cqg_ensemble_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
-    "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP]),
+    "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
+    "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
     "cqg_ensemble_destroy": (C.c_int, [_P]),
     "cqg_model_create": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(_P)]),
     "cqg_model_desc": (C.c_int, [_P, C.POINTER(C.POINTER(cqg_system_desc))]),

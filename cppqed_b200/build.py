@@ -1,0 +1,107 @@
+"""Builds the engine library ``cppqed_b200/_lib/libcqg.so`` for sm_100a.
+
+The host sources (element library, model builder, lowering, errors) are compiled
+with g++, the CUDA sources with nvcc (``-gencode arch=compute_100a,code=sm_100a``),
+and everything is linked into one shared library exporting the C ABI of
+``include/cqg.h`` and ``include/cqg_model.h``.  Rebuilds only what is out of date.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+OBJDIR = os.path.join(HERE, "_build")
+LIB = os.path.join(LIBDIR, "libcqg.so")
+
+HOST_SOURCES = ["host/tridiagonal.cpp", "host/elements.cpp", "host/model.cpp", "host/pars.cpp",
+                "host/scripts.cpp", "host/errors.cpp", "host/api_model.cpp", "host/lowering.cpp"]
+CUDA_SOURCES = ["cuda/api.cu"]
+# the kernel instantiations: one object per (precision, rows per lane)
+KERNEL_INSTANCES = [(r, e) for r in ("double", "float") for e in (1, 2, 4)]
+HEADERS = ["cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
+           "host/elements.hpp", "host/tridiagonal.hpp", "host/pars.hpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc():
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else "nvcc"
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("build step failed: " + " ".join(cmd[:3]) + " ...")
+    return r.stdout + r.stderr
+
+
+def build(verbose=False, ptxas_info=False):
+    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    inc = ["-I" + os.path.join(ROOT, "include")]
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
+                                                          for h in ("cqg.h", "cqg_model.h")]
+    objs = []
+    for src in HOST_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        if _stale(o, [s] + headers):
+            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", *inc, "-c", s, "-o", o], verbose)
+        objs.append(o)
+    info = ""
+    jobs = []
+    for src in CUDA_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
+        jobs.append((s, o, []))
+    inst = os.path.join(CSRC, "cuda", "kernels_inst.cu")
+    for r, e in KERNEL_INSTANCES:
+        jobs.append((inst, os.path.join(OBJDIR, "kernels_%s_e%d.o" % (r, e)),
+                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e]))
+    procs = []
+    for s, o, defs in jobs:
+        objs.append(o)
+        if _stale(o, [s] + headers) or ptxas_info:
+            cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs, "-c", s,
+                   "-o", o]
+            if ptxas_info:
+                cmd.insert(1, "-Xptxas=-v")
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    for cmd, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out)
+            raise RuntimeError("build step failed: " + " ".join(cmd[:3]) + " ...")
+        info += out
+    if _stale(LIB, objs):
+        _run([_nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], verbose)
+    return info
+
+
+def build_oracle(verbose=False):
+    """Builds the CPU oracle (test infrastructure) with its Makefile."""
+    out = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "PYTHON=" + sys.executable], verbose)
+    return out
+
+
+if __name__ == "__main__":
+    txt = build(verbose=True, ptxas_info="--ptxas-info" in sys.argv)
+    if txt:
+        print(txt)
+    build_oracle(verbose=True)

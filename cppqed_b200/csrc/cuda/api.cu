@@ -1,0 +1,794 @@
+// extern "C" engine entry points (include/cqg.h): device-resident systems, ensembles
+// and the launches of the fused MCWF kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../host/errors.hpp"
+#include "../host/lowering.hpp"
+#include "cqg.h"
+#include "mcwf_kernel.cuh"
+
+using cqg::fail;
+using cqg::guarded;
+namespace dev = cqg::dev;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename F>
+int guardedCuda(F&& f) {
+  return guarded([&]() -> int {
+    try {
+      return f();
+    } catch (const CudaError& e) {
+      return fail(CQG_E_CUDA, e.what());
+    }
+  });
+}
+
+// single device allocation carved into aligned sub-buffers
+struct Arena {
+  std::vector<std::pair<size_t, size_t>> parts;  // offset, size
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    const size_t off = (total + 255) & ~size_t(255);
+    total = off + bytes;
+    return off;
+  }
+};
+
+}  // namespace
+
+struct cqg_system {
+  cqg::LoweredSystem L;
+  int device = 0;
+  void* dmem = nullptr;
+  dev::SysDev sd{};
+  ~cqg_system() {
+    if (dmem) cudaFree(dmem);
+  }
+};
+
+struct cqg_ensemble {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evRun0 = nullptr, evRun1 = nullptr;
+  float lastMs = 0, lastRunMs = 0;
+  int64_t nTraj = 0;
+  int nAvrMax = 0, Dmax = 0, Smax = 0;
+  cqg_mcwf_pars pars{};
+  std::vector<const cqg_system*> systems;
+  std::vector<int> sysIdx;
+  std::vector<long long> psiOff;
+  size_t elemBytes = 16;
+  // device buffers
+  void* dmem = nullptr;
+  dev::TrajDev td{};
+  dev::SysDev* dSystems = nullptr;
+  int* dQueue = nullptr;
+  int* dOrder = nullptr;
+  unsigned* dStatusOr = nullptr;
+  double* dAvr = nullptr;
+  size_t avrCap = 0;
+  double* dSums = nullptr;
+  size_t sumsCap = 0;
+  int jumpCap = 64;
+  ~cqg_ensemble() {
+    if (dAvr) cudaFree(dAvr);
+    if (dSums) cudaFree(dSums);
+    if (dmem) cudaFree(dmem);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (evRun0) cudaEventDestroy(evRun0);
+    if (evRun1) cudaEventDestroy(evRun1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+using dcomp = std::complex<double>;
+
+// rates of the initial state (the MCWF_Trajectory constructor, MCWF_Trajectory.h:114-117)
+std::vector<double> hostRates(const cqg::LoweredSystem& L, const std::vector<dcomp>& psi) {
+  std::vector<double> r(L.jumps.size());
+  for (size_t m = 0; m < L.jumps.size(); ++m) {
+    if (!L.weights[m].empty()) {
+      double s = 0;
+      for (int64_t i = 0; i < L.D; ++i) s += L.weights[m][i] * std::norm(psi[i]);
+      r[m] = s;
+    } else {
+      const auto& J = L.jumps[m];
+      double s = 0;
+      for (int64_t i = 0; i < L.D; ++i) {
+        dcomp acc = 0;
+        for (int k = 0; k < J.S; ++k) acc += J.val[k * L.D + i] * psi[J.col[k * L.D + i]];
+        s += std::norm(acc);
+      }
+      r[m] = s;
+    }
+  }
+  return r;
+}
+
+template <typename T>
+void upload(void* base, size_t off, const std::vector<T>& v) {
+  if (!v.empty()) ck(cudaMemcpy(static_cast<char*>(base) + off, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+std::vector<double2> toD2(const std::vector<dcomp>& v) {
+  std::vector<double2> r(v.size());
+  for (size_t i = 0; i < v.size(); ++i) r[i] = make_double2(v[i].real(), v[i].imag());
+  return r;
+}
+std::vector<float2> toF2(const std::vector<dcomp>& v) {
+  std::vector<float2> r(v.size());
+  for (size_t i = 0; i < v.size(); ++i) r[i] = make_float2(float(v[i].real()), float(v[i].imag()));
+  return r;
+}
+
+void buildSystemDevice(cqg_system& s) {
+  const auto& L = s.L;
+  const int64_t D = L.D;
+  Arena A;
+  const int nJ = int(L.jumps.size()), nObs = int(L.obs.size());
+  int SJ = 0, SO = 0;
+  for (auto& j : L.jumps) SJ = std::max(SJ, j.S);
+  for (auto& o : L.obs) SO = std::max(SO, o.S);
+  // pack jump and observable tables to common slot counts
+  std::vector<int> jcol(size_t(nJ) * SJ * D), ocol(size_t(nObs) * SO * D);
+  std::vector<dcomp> jval(size_t(nJ) * SJ * D), oval(size_t(nObs) * SO * D);
+  std::vector<double> jw(size_t(nJ) * D, 0.);
+  std::vector<int> jHasW(nJ), oRe(nObs), oIm(nObs);
+  for (int m = 0; m < nJ; ++m) {
+    const auto& J = L.jumps[m];
+    for (int k = 0; k < SJ; ++k)
+      for (int64_t r = 0; r < D; ++r) {
+        const size_t o = (size_t(m) * SJ + k) * D + r;
+        jcol[o] = k < J.S ? J.col[k * D + r] : int(r);
+        jval[o] = k < J.S ? J.val[k * D + r] : dcomp(0, 0);
+      }
+    jHasW[m] = L.weights[m].empty() ? 0 : 1;
+    if (jHasW[m]) std::copy(L.weights[m].begin(), L.weights[m].end(), jw.begin() + size_t(m) * D);
+  }
+  for (int q = 0; q < nObs; ++q) {
+    const auto& O = L.obs[q];
+    for (int k = 0; k < SO; ++k)
+      for (int64_t r = 0; r < D; ++r) {
+        const size_t o = (size_t(q) * SO + k) * D + r;
+        ocol[o] = k < O.S ? O.col[k * D + r] : int(r);
+        oval[o] = k < O.S ? O.val[k * D + r] : dcomp(0, 0);
+      }
+    oRe[q] = L.obsColRe[q];
+    oIm[q] = L.obsColIm[q];
+  }
+  const auto& H = L.ham;
+  const int S = H.S;
+  const size_t oCol = A.add(H.col.size() * 4 + 4), oJcol = A.add(jcol.size() * 4 + 4), oJw = A.add(jw.size() * 8 + 8),
+               oJHasW = A.add(jHasW.size() * 4 + 4), oOcol = A.add(ocol.size() * 4 + 4),
+               oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4),
+               oFreq = A.add(H.freq.size() * 16 + 16), oLambda = A.add(L.lambda.size() * 16 + 16),
+               oDiagD = A.add(H.diag.size() * 16 + 16), oValD = A.add(H.val.size() * 16 + 16),
+               oJvalD = A.add(jval.size() * 16 + 16), oDiagF = A.add(H.diag.size() * 8 + 8),
+               oValF = A.add(H.val.size() * 8 + 8), oJvalF = A.add(jval.size() * 8 + 8);
+  ck(cudaMalloc(&s.dmem, A.total), "cudaMalloc(system)");
+  char* b = static_cast<char*>(s.dmem);
+  upload(b, oCol, H.col);
+  upload(b, oJcol, jcol);
+  upload(b, oJw, jw);
+  upload(b, oJHasW, jHasW);
+  upload(b, oOcol, ocol);
+  upload(b, oOval, toD2(oval));
+  upload(b, oORe, oRe);
+  upload(b, oOIm, oIm);
+  upload(b, oFreq, toD2(H.freq));
+  upload(b, oLambda, toD2(L.lambda));
+  upload(b, oDiagD, toD2(H.diag));
+  upload(b, oValD, toD2(H.val));
+  upload(b, oJvalD, toD2(jval));
+  upload(b, oDiagF, toF2(H.diag));
+  upload(b, oValF, toF2(H.val));
+  upload(b, oJvalF, toF2(jval));
+  auto& sd = s.sd;
+  sd.D = int(D);
+  sd.S = S;
+  sd.SJ = SJ;
+  sd.SO = SO;
+  sd.nJ = nJ;
+  sd.nObs = nObs;
+  sd.nAvr = L.nAvr;
+  sd.hasH = L.hasH ? 1 : 0;
+  sd.hasEx = L.hasEx ? 1 : 0;
+  sd.hasFreq = H.freq.empty() ? 0 : 1;
+  sd.col = reinterpret_cast<const int*>(b + oCol);
+  sd.jcol = reinterpret_cast<const int*>(b + oJcol);
+  sd.jw = reinterpret_cast<const double*>(b + oJw);
+  sd.jHasW = reinterpret_cast<const int*>(b + oJHasW);
+  sd.ocol = reinterpret_cast<const int*>(b + oOcol);
+  sd.oval = reinterpret_cast<const double2*>(b + oOval);
+  sd.oRe = reinterpret_cast<const int*>(b + oORe);
+  sd.oIm = reinterpret_cast<const int*>(b + oOIm);
+  sd.freq = H.freq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFreq);
+  sd.lambda = L.lambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oLambda);
+  sd.diagD = reinterpret_cast<const double2*>(b + oDiagD);
+  sd.valD = reinterpret_cast<const double2*>(b + oValD);
+  sd.jvalD = reinterpret_cast<const double2*>(b + oJvalD);
+  sd.diagF = reinterpret_cast<const float2*>(b + oDiagF);
+  sd.valF = reinterpret_cast<const float2*>(b + oValF);
+  sd.jvalF = reinterpret_cast<const float2*>(b + oJvalF);
+}
+
+// ---- kernel dispatch -------------------------------------------------------------
+
+using KernelFn = void (*)(dev::TrajDev, dev::RunArgs);
+
+}  // namespace
+
+namespace cqg {
+namespace dev {
+KernelFn pick_double_e1(int smax);
+KernelFn pick_double_e2(int smax);
+KernelFn pick_double_e4(int smax);
+KernelFn pick_float_e1(int smax);
+KernelFn pick_float_e2(int smax);
+KernelFn pick_float_e4(int smax);
+}  // namespace dev
+}  // namespace cqg
+
+namespace {
+
+KernelFn pickKernel(bool fp64, int E, int SMAX) {
+  if (fp64) return E == 1 ? dev::pick_double_e1(SMAX) : E == 2 ? dev::pick_double_e2(SMAX) : dev::pick_double_e4(SMAX);
+  return E == 1 ? dev::pick_float_e1(SMAX) : E == 2 ? dev::pick_float_e2(SMAX) : dev::pick_float_e4(SMAX);
+}
+
+__global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, int nAvrStride, int nAvr,
+                                     double* __restrict__ sums) {
+  // one block per (output, column): fixed-order strided sums then a fixed tree
+  const int k = blockIdx.x / nAvr, c = blockIdx.x % nAvr;
+  __shared__ double part[256];
+  double acc = 0.;
+  for (int i = threadIdx.x; i < nTraj; i += blockDim.x) acc += avr[((size_t)k * nTraj + i) * nAvrStride + c];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o; o >>= 1) {
+    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[(size_t)k * nAvr + c] = part[0];
+}
+
+__global__ void statusOrKernel(const unsigned* __restrict__ st, int n, unsigned* out) {
+  unsigned v = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v |= st[i];
+  v = __reduce_or_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && v) atomicOr(out, v);
+}
+
+int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sysIndex, const cqg_complex* psi0s,
+                   const int64_t* psi0Off, int64_t nTraj, const cqg_mcwf_pars* pars, cqg_ensemble** out) {
+  if (!systems || nSys < 1 || !psi0s || nTraj < 1 || !pars || !out)
+    return fail(CQG_E_INVALID, "ensemble: null argument or empty ensemble");
+  if (nTraj > (int64_t(1) << 30)) return fail(CQG_E_INVALID, "ensemble: too many trajectories");
+  if (pars->precision != CQG_FP64 && pars->precision != CQG_FP32) return fail(CQG_E_INVALID, "ensemble: bad precision");
+  if (pars->rng != CQG_RNG_PCG64 && pars->rng != CQG_RNG_PHILOX) return fail(CQG_E_INVALID, "ensemble: bad rng");
+  if (!(pars->eps_rel > 0) || !(pars->eps_abs >= 0) || !(pars->dp_limit > 0) || !(pars->overshoot_tolerance >= 1))
+    return fail(CQG_E_INVALID, "ensemble: eps_rel > 0, eps_abs >= 0, dp_limit > 0, overshoot_tolerance >= 1 required");
+  auto e = std::make_unique<cqg_ensemble>();
+  e->nTraj = nTraj;
+  e->pars = *pars;
+  if (e->pars.max_attempts <= 0) e->pars.max_attempts = 100000;
+  for (int s = 0; s < nSys; ++s) {
+    if (!systems[s]) return fail(CQG_E_INVALID, "ensemble: null system");
+    e->systems.push_back(systems[s]);
+    e->Dmax = std::max<int>(e->Dmax, int(systems[s]->L.D));
+    e->Smax = std::max<int>(e->Smax, systems[s]->sd.S);
+    e->nAvrMax = std::max<int>(e->nAvrMax, systems[s]->L.nAvr);
+    if (int(systems[s]->L.jumps.size()) > dev::MAX_JUMPS)
+      return fail(CQG_E_UNSUPPORTED, "ensemble: more than 8 jump operators");
+  }
+  if (e->Dmax > 128) return fail(CQG_E_UNSUPPORTED, "ensemble: total dimension above 128 is not supported by the warp kernel");
+  if (e->Smax > 8) return fail(CQG_E_UNSUPPORTED, "ensemble: more than 8 off-diagonal entries per row");
+  e->device = systems[0]->device;
+  ck(cudaSetDevice(e->device), "cudaSetDevice");
+  ck(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaEventCreate(&e->ev0), "cudaEventCreate");
+  ck(cudaEventCreate(&e->ev1), "cudaEventCreate");
+  ck(cudaEventCreate(&e->evRun0), "cudaEventCreate");
+  ck(cudaEventCreate(&e->evRun1), "cudaEventCreate");
+  e->elemBytes = pars->precision == CQG_FP64 ? 16 : 8;
+
+  e->sysIdx.resize(nTraj);
+  e->psiOff.resize(nTraj);
+  long long off = 0;
+  for (int64_t i = 0; i < nTraj; ++i) {
+    const int si = sysIndex ? sysIndex[i] : 0;
+    if (si < 0 || si >= nSys) return fail(CQG_E_INVALID, "ensemble: system index out of range");
+    e->sysIdx[i] = si;
+    e->psiOff[i] = off;
+    off += systems[si]->L.D;
+  }
+  const long long psiElems = off;
+
+  Arena A;
+  const size_t oPsi = A.add(size_t(psiElems) * e->elemBytes), oOff = A.add(nTraj * 8), oIdx = A.add(nTraj * 4),
+               oT = A.add(nTraj * 8), oT0 = A.add(nTraj * 8), oTry = A.add(nTraj * 8), oDid = A.add(nTraj * 8),
+               oRng = A.add(nTraj * 32), oCnt = A.add(nTraj * 64), oMax = A.add(nTraj * 24), oSt = A.add(nTraj * 4),
+               oJT = A.add(nTraj * e->jumpCap * 8), oJL = A.add(nTraj * e->jumpCap * 4), oJN = A.add(nTraj * 8),
+               oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(16), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
+  ck(cudaMalloc(&e->dmem, A.total), "cudaMalloc(ensemble)");
+  ck(cudaMemset(e->dmem, 0, A.total), "cudaMemset");
+  char* b = static_cast<char*>(e->dmem);
+
+  // host-side initial values
+  std::vector<double> t(nTraj, 0.), t0(nTraj, 0.), dtTry(nTraj), dtDid(nTraj, 0.);
+  std::vector<unsigned long long> rng(4 * nTraj, 0), cnt(8 * nTraj, 0);
+  std::vector<unsigned char> psiBytes(size_t(psiElems) * e->elemBytes);
+  std::vector<double> initRates;
+  for (int64_t i = 0; i < nTraj; ++i) {
+    const cqg_system* s = systems[e->sysIdx[i]];
+    const int64_t D = s->L.D;
+    const cqg_complex* p = psi0s + (psi0Off ? psi0Off[i] : 0);
+    std::vector<dcomp> psi(D);
+    for (int64_t k = 0; k < D; ++k) psi[k] = dcomp(p[k].re, p[k].im);
+    for (int64_t k = 0; k < D; ++k) {
+      if (e->elemBytes == 16) {
+        double2 v = make_double2(psi[k].real(), psi[k].imag());
+        std::memcpy(&psiBytes[(e->psiOff[i] + k) * 16], &v, 16);
+      } else {
+        float2 v = make_float2(float(psi[k].real()), float(psi[k].imag()));
+        std::memcpy(&psiBytes[(e->psiOff[i] + k) * 8], &v, 8);
+      }
+    }
+    double dt0 = pars->dt_init > 0 ? pars->dt_init : 1. / (10. * s->L.highestFrequency);
+    if (pars->rng == CQG_RNG_PCG64) {
+      const auto g = dev::Pcg64::seeded(pars->seed, pars->prng_stream + uint64_t(i));
+      rng[4 * i + 0] = g.state.hi;
+      rng[4 * i + 1] = g.state.lo;
+      rng[4 * i + 2] = g.inc.hi;
+      rng[4 * i + 3] = g.inc.lo;
+    }
+    // MCWF_Trajectory constructor: dpLimit should not be overshot at startup either
+    if (pars->noise && !s->L.jumps.empty()) {
+      if (psi0Off || i == 0) initRates = hostRates(s->L, psi);
+      double totalRate = 0.;
+      for (double r : initRates) totalRate += r;
+      const double suggested = pars->dp_limit / totalRate;
+      if (totalRate * dt0 > pars->dp_limit) cnt[8 * i + 4] += 1;
+      dt0 = s->L.hasH ? std::min(dt0, suggested) : suggested;
+    }
+    dtTry[i] = dt0;
+  }
+  ck(cudaMemcpy(b + oPsi, psiBytes.data(), psiBytes.size(), cudaMemcpyHostToDevice), "cudaMemcpy(psi)");
+  upload(b, oOff, e->psiOff);
+  upload(b, oIdx, e->sysIdx);
+  upload(b, oT, t);
+  upload(b, oT0, t0);
+  upload(b, oTry, dtTry);
+  upload(b, oDid, dtDid);
+  upload(b, oRng, rng);
+  upload(b, oCnt, cnt);
+  std::vector<dev::SysDev> sds;
+  for (auto* s : e->systems) sds.push_back(s->sd);
+  upload(b, oSys, sds);
+
+  auto& td = e->td;
+  td.nTraj = int(nTraj);
+  td.sysIdx = reinterpret_cast<const int*>(b + oIdx);
+  td.systems = reinterpret_cast<const dev::SysDev*>(b + oSys);
+  td.psi = b + oPsi;
+  td.psiOff = reinterpret_cast<const long long*>(b + oOff);
+  td.t = reinterpret_cast<double*>(b + oT);
+  td.t0 = reinterpret_cast<double*>(b + oT0);
+  td.dtTry = reinterpret_cast<double*>(b + oTry);
+  td.dtDid = reinterpret_cast<double*>(b + oDid);
+  td.rng = reinterpret_cast<unsigned long long*>(b + oRng);
+  td.cnt = reinterpret_cast<unsigned long long*>(b + oCnt);
+  td.maxima = reinterpret_cast<double*>(b + oMax);
+  td.status = reinterpret_cast<unsigned*>(b + oSt);
+  td.jumpT = reinterpret_cast<double*>(b + oJT);
+  td.jumpL = reinterpret_cast<int*>(b + oJL);
+  td.jumpN = reinterpret_cast<unsigned long long*>(b + oJN);
+  td.jumpCap = e->jumpCap;
+  e->dSystems = reinterpret_cast<dev::SysDev*>(b + oSys);
+  e->dQueue = reinterpret_cast<int*>(b + oQ);
+  e->dOrder = reinterpret_cast<int*>(b + oOrd);
+  e->dStatusOr = reinterpret_cast<unsigned*>(b + oSOr);
+  // longest trajectories first (dimension as the cost proxy) for the work queue
+  std::vector<int> order(nTraj);
+  std::iota(order.begin(), order.end(), 0);
+  if (nSys > 1)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+      return systems[e->sysIdx[a]]->L.D > systems[e->sysIdx[c]]->L.D;
+    });
+  upload(b, oOrd, order);
+  *out = e.release();
+  return CQG_OK;
+}
+
+int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
+  ck(cudaSetDevice(e->device), "cudaSetDevice");
+  const int nAvr = e->nAvrMax + 1;  // the linear averages, then dtDid
+  const size_t need = size_t(std::max(nOut, 1)) * e->nTraj * nAvr;
+  if (need > e->avrCap) {
+    if (e->dAvr) cudaFree(e->dAvr);
+    e->dAvr = nullptr;
+    ck(cudaMalloc(&e->dAvr, need * sizeof(double)), "cudaMalloc(averages)");
+    e->avrCap = need;
+  }
+  const size_t needS = size_t(std::max(nOut, 1)) * nAvr;
+  if (needS > e->sumsCap) {
+    if (e->dSums) cudaFree(e->dSums);
+    e->dSums = nullptr;
+    ck(cudaMalloc(&e->dSums, needS * sizeof(double)), "cudaMalloc(sums)");
+    e->sumsCap = needS;
+  }
+  ck(cudaEventRecord(e->evRun0, e->stream), "cudaEventRecord");
+  ck(cudaMemsetAsync(e->dAvr, 0, need * sizeof(double), e->stream), "cudaMemsetAsync");
+  ck(cudaMemsetAsync(e->dQueue, 0, sizeof(int), e->stream), "cudaMemsetAsync");
+  ck(cudaMemsetAsync(e->dStatusOr, 0, sizeof(unsigned), e->stream), "cudaMemsetAsync");
+  ra.avrOut = e->dAvr;
+  ra.nAvrStride = nAvr;
+  ra.queue = e->dQueue;
+  ra.order = e->systems.size() > 1 ? e->dOrder : nullptr;
+  ra.absSlot = e->pars.eps_rel;  // make_controlled(epsRel, epsAbs, ...) (ODE.h:205)
+  ra.relSlot = e->pars.eps_abs;
+  ra.dpLimit = e->pars.dp_limit;
+  ra.overTol = e->pars.overshoot_tolerance;
+  ra.maxAttempts = e->pars.max_attempts;
+  ra.noise = e->pars.noise;
+  ra.rng = e->pars.rng;
+  ra.seed = e->pars.seed;
+  ra.maxStepsPerInterval = 2000000000LL;
+  ra.timeLimitNs = 120ull * 1000000000ull;
+
+  const int E = e->Dmax <= 32 ? 1 : e->Dmax <= 64 ? 2 : 4;
+  const int SM = e->Smax <= 2 ? 2 : e->Smax <= 4 ? 4 : 8;
+  KernelFn fn = pickKernel(e->pars.precision == CQG_FP64, E, SM);
+  const int threads = 128;
+  const size_t smem = size_t(threads / 32) * 3 * 32 * E * e->elemBytes;
+  ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+     "cudaFuncSetAttribute");
+  int perSM = 0, nSM = 0;
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem), "occupancy");
+  ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e->device), "attribute");
+  const int64_t warpsNeeded = e->nTraj;
+  int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (warpsNeeded + 3) / 4));
+  grid = std::max(grid, 1);
+  ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
+  {
+    dev::TrajDev tdArg = e->td;
+    void* args[] = {&tdArg, &ra};
+    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(threads), args, smem, e->stream),
+       "kernel launch");
+  }
+  ck(cudaEventRecord(e->ev1, e->stream), "cudaEventRecord");
+  if (nAvr > 0 && nOut > 0) {
+    reduceAveragesKernel<<<nOut * nAvr, 256, 0, e->stream>>>(e->dAvr, int(e->nTraj), ra.nAvrStride, nAvr, e->dSums);
+    ck(cudaGetLastError(), "reduce launch");
+  }
+  statusOrKernel<<<std::max(1, std::min(148, int((e->nTraj + 255) / 256))), 256, 0, e->stream>>>(
+      e->td.status, int(e->nTraj), e->dStatusOr);
+  ck(cudaGetLastError(), "status launch");
+  unsigned bits = 0;
+  ck(cudaMemcpyAsync(&bits, e->dStatusOr, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream), "cudaMemcpyAsync");
+  std::vector<double> sums;
+  if (avrHost && nAvr > 0 && nOut > 0) {
+    ck(cudaMemcpyAsync(avrHost, e->dSums, size_t(nOut) * nAvr * sizeof(double), cudaMemcpyDeviceToHost, e->stream),
+       "cudaMemcpyAsync");
+  }
+  ck(cudaEventRecord(e->evRun1, e->stream), "cudaEventRecord");
+  ck(cudaStreamSynchronize(e->stream), "kernel execution");
+  ck(cudaEventElapsedTime(&e->lastMs, e->ev0, e->ev1), "cudaEventElapsedTime");
+  ck(cudaEventElapsedTime(&e->lastRunMs, e->evRun0, e->evRun1), "cudaEventElapsedTime");
+  if (bits & 3u) return fail(CQG_E_NONFINITE, "a trajectory produced a non-finite norm or rate");
+  if (bits & 12u) return fail(CQG_E_STALLED, "a trajectory exhausted its step-size or attempt budget");
+  return CQG_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// FMA-chain probe: each thread runs `iters` dependent-free FMA groups on 8 accumulators
+template <typename R>
+__global__ void fmaProbeKernel(R* out, int iters, R a, R b) {
+  R x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = R(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  R s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == R(-1.2345)) out[threadIdx.x] = s;  // keeps the loop alive
+}
+
+template <typename R>
+double probe(int device) {
+  int nSM = 0;
+  ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device), "attribute");
+  R* out = nullptr;
+  ck(cudaMalloc(&out, 1024 * sizeof(R)), "cudaMalloc");
+  cudaEvent_t a, b;
+  ck(cudaEventCreate(&a), "event");
+  ck(cudaEventCreate(&b), "event");
+  const int blocks = nSM * 8, threads = 256, iters = 4096;
+  fmaProbeKernel<R><<<blocks, threads>>>(out, iters, R(0.999999), R(1e-7));
+  ck(cudaEventRecord(a), "event");
+  const int reps = 5;
+  for (int r = 0; r < reps; ++r) fmaProbeKernel<R><<<blocks, threads>>>(out, iters, R(0.999999), R(1e-7));
+  ck(cudaEventRecord(b), "event");
+  ck(cudaEventSynchronize(b), "sync");
+  float ms = 0;
+  ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  const double flops = 2.0 * 8 * double(iters) * blocks * threads * reps;
+  return flops / (ms * 1e-3) / 1e12;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cqg_device_count(int* count) {
+  if (!count) return fail(CQG_E_INVALID, "null argument");
+  int n = 0;
+  const cudaError_t err = cudaGetDeviceCount(&n);
+  if (err != cudaSuccess) {
+    *count = 0;
+    cudaGetLastError();
+    return fail(CQG_E_NODEVICE, std::string("no CUDA device: ") + cudaGetErrorString(err));
+  }
+  *count = n;
+  return CQG_OK;
+}
+
+int cqg_system_create(const cqg_system_desc* desc, cqg_system** out) {
+  return guardedCuda([&] {
+    if (!desc || !out) return fail(CQG_E_INVALID, "cqg_system_create: null argument");
+    int n = 0;
+    if (cqg_device_count(&n) != CQG_OK || n < 1) return fail(CQG_E_NODEVICE, "cqg_system_create: no CUDA device");
+    auto s = std::make_unique<cqg_system>();
+    s->L = cqg::lowerSystem(*desc);
+    if (!(s->L.highestFrequency > 0) && s->L.hasH)
+      return fail(CQG_E_INVALID, "cqg_system_create: highest_frequency must be positive");
+    ck(cudaGetDevice(&s->device), "cudaGetDevice");
+    buildSystemDevice(*s);
+    *out = s.release();
+    return CQG_OK;
+  });
+}
+
+int cqg_system_dimension(const cqg_system* sys, int64_t* d) {
+  if (!sys || !d) return fail(CQG_E_INVALID, "null argument");
+  *d = sys->L.D;
+  return CQG_OK;
+}
+
+int cqg_system_destroy(cqg_system* sys) {
+  delete sys;
+  return CQG_OK;
+}
+
+int cqg_ensemble_create(const cqg_system* sys, const cqg_complex* psi0, int64_t n_traj, const cqg_mcwf_pars* pars,
+                        cqg_ensemble** out) {
+  return guardedCuda([&] { return createEnsemble(&sys, 1, nullptr, psi0, nullptr, n_traj, pars, out); });
+}
+
+int cqg_batch_create(const cqg_system* const* systems, int32_t n_systems, const int32_t* sys_index,
+                     const cqg_complex* psi0s, const int64_t* psi0_offsets, int64_t n_traj, const cqg_mcwf_pars* pars,
+                     cqg_ensemble** out) {
+  return guardedCuda([&] {
+    if (!sys_index || !psi0_offsets) return fail(CQG_E_INVALID, "cqg_batch_create: null index arrays");
+    return createEnsemble(systems, n_systems, sys_index, psi0s, psi0_offsets, n_traj, pars, out);
+  });
+}
+
+int cqg_ensemble_run(cqg_ensemble* ens, double Dt, int32_t n_intervals, double* avr_out) {
+  return guardedCuda([&] {
+    if (!ens || !(Dt > 0) || n_intervals < 1) return fail(CQG_E_INVALID, "cqg_ensemble_run: Dt > 0 and n_intervals >= 1 required");
+    dev::RunArgs ra{};
+    ra.mode = dev::RUN_INTERVALS;
+    ra.Dt = Dt;
+    ra.nIntervals = n_intervals;
+    return launchRun(ens, ra, n_intervals, avr_out);
+  });
+}
+
+int cqg_ensemble_advance_to(cqg_ensemble* ens, double t_end, double* avr_out) {
+  return guardedCuda([&] {
+    if (!ens) return fail(CQG_E_INVALID, "null ensemble");
+    dev::RunArgs ra{};
+    ra.mode = dev::RUN_TO;
+    ra.tEnd = t_end;
+    ra.nIntervals = 1;
+    return launchRun(ens, ra, 1, avr_out);
+  });
+}
+
+int cqg_ensemble_steps(cqg_ensemble* ens, int32_t n_steps, double T, double* avr_out) {
+  return guardedCuda([&] {
+    if (!ens || n_steps < 0) return fail(CQG_E_INVALID, "cqg_ensemble_steps: n_steps >= 0 required");
+    dev::RunArgs ra{};
+    ra.mode = dev::RUN_STEPS;
+    ra.nSteps = n_steps;
+    ra.T = T;
+    ra.nIntervals = 1;
+    return launchRun(ens, ra, 1, avr_out);
+  });
+}
+
+int cqg_ensemble_traj_averages(cqg_ensemble* ens, double* out) {
+  return guardedCuda([&] {
+    if (!ens || !out) return fail(CQG_E_INVALID, "null argument");
+    // the per-trajectory slots of the last output of the last run
+    if (!ens->dAvr) return fail(CQG_E_INVALID, "cqg_ensemble_traj_averages: no run yet");
+    ck(cudaMemcpy(out, ens->dAvr, size_t(ens->nTraj) * (ens->nAvrMax + 1) * sizeof(double), cudaMemcpyDeviceToHost),
+       "cudaMemcpy");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_size(const cqg_ensemble* ens, int64_t* n_traj, int32_t* n_avr) {
+  if (!ens) return fail(CQG_E_INVALID, "null ensemble");
+  if (n_traj) *n_traj = ens->nTraj;
+  if (n_avr) *n_avr = ens->nAvrMax;
+  return CQG_OK;
+}
+
+int cqg_ensemble_get_state(const cqg_ensemble* ens, int64_t i, cqg_complex* psi) {
+  return guardedCuda([&] {
+    if (!ens || !psi || i < 0 || i >= ens->nTraj) return fail(CQG_E_INVALID, "cqg_ensemble_get_state: bad index");
+    const int64_t D = ens->systems[ens->sysIdx[i]]->L.D;
+    std::vector<unsigned char> b(D * ens->elemBytes);
+    ck(cudaMemcpy(b.data(), static_cast<char*>(ens->td.psi) + ens->psiOff[i] * ens->elemBytes, b.size(),
+                  cudaMemcpyDeviceToHost),
+       "cudaMemcpy");
+    for (int64_t k = 0; k < D; ++k) {
+      if (ens->elemBytes == 16) {
+        double2 v;
+        std::memcpy(&v, &b[k * 16], 16);
+        psi[k] = {v.x, v.y};
+      } else {
+        float2 v;
+        std::memcpy(&v, &b[k * 8], 8);
+        psi[k] = {double(v.x), double(v.y)};
+      }
+    }
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_set_state(cqg_ensemble* ens, int64_t i, const cqg_complex* psi) {
+  return guardedCuda([&] {
+    if (!ens || !psi || i < 0 || i >= ens->nTraj) return fail(CQG_E_INVALID, "cqg_ensemble_set_state: bad index");
+    const int64_t D = ens->systems[ens->sysIdx[i]]->L.D;
+    std::vector<unsigned char> b(D * ens->elemBytes);
+    for (int64_t k = 0; k < D; ++k) {
+      if (ens->elemBytes == 16) {
+        double2 v = make_double2(psi[k].re, psi[k].im);
+        std::memcpy(&b[k * 16], &v, 16);
+      } else {
+        float2 v = make_float2(float(psi[k].re), float(psi[k].im));
+        std::memcpy(&b[k * 8], &v, 8);
+      }
+    }
+    ck(cudaMemcpy(static_cast<char*>(ens->td.psi) + ens->psiOff[i] * ens->elemBytes, b.data(), b.size(),
+                  cudaMemcpyHostToDevice),
+       "cudaMemcpy");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_get_times(const cqg_ensemble* ens, double* t, double* dt_did, double* dt_try) {
+  return guardedCuda([&] {
+    if (!ens) return fail(CQG_E_INVALID, "null ensemble");
+    const size_t n = size_t(ens->nTraj) * sizeof(double);
+    if (t) ck(cudaMemcpy(t, ens->td.t, n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (dt_did) ck(cudaMemcpy(dt_did, ens->td.dtDid, n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (dt_try) ck(cudaMemcpy(dt_try, ens->td.dtTry, n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_get_counters(const cqg_ensemble* ens, uint64_t* counters) {
+  return guardedCuda([&] {
+    if (!ens || !counters) return fail(CQG_E_INVALID, "null argument");
+    ck(cudaMemcpy(counters, ens->td.cnt, size_t(ens->nTraj) * 64, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_norm_dev) {
+  return guardedCuda([&] {
+    if (!ens) return fail(CQG_E_INVALID, "null ensemble");
+    std::vector<double> m(3 * ens->nTraj);
+    ck(cudaMemcpy(m.data(), ens->td.maxima, m.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    for (int64_t i = 0; i < ens->nTraj; ++i) {
+      if (max_overshoot) max_overshoot[i] = m[3 * i];
+      if (max_norm_dev) max_norm_dev[i] = m[3 * i + 2];
+    }
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_get_jumps(const cqg_ensemble* ens, int64_t i, int32_t cap, double* times, int32_t* lindblads,
+                           int32_t* n_out) {
+  return guardedCuda([&] {
+    if (!ens || i < 0 || i >= ens->nTraj || cap < 0) return fail(CQG_E_INVALID, "cqg_ensemble_get_jumps: bad argument");
+    unsigned long long n = 0;
+    ck(cudaMemcpy(&n, ens->td.jumpN + i, 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    const int J = ens->jumpCap;
+    std::vector<double> tt(J);
+    std::vector<int> ll(J);
+    ck(cudaMemcpy(tt.data(), ens->td.jumpT + size_t(i) * J, J * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    ck(cudaMemcpy(ll.data(), ens->td.jumpL + size_t(i) * J, J * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    const unsigned long long kept = std::min<unsigned long long>(n, J);
+    const unsigned long long first = n - kept;
+    int32_t w = 0;
+    for (unsigned long long k = first; k < n && w < cap; ++k, ++w) {
+      if (times) times[w] = tt[k % J];
+      if (lindblads) lindblads[w] = ll[k % J];
+    }
+    if (n_out) *n_out = w;
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_status(const cqg_ensemble* ens, uint32_t* bits) {
+  return guardedCuda([&] {
+    if (!ens || !bits) return fail(CQG_E_INVALID, "null argument");
+    std::vector<unsigned> st(ens->nTraj);
+    ck(cudaMemcpy(st.data(), ens->td.status, st.size() * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    unsigned b = 0;
+    for (auto v : st) b |= v;
+    *bits = b;
+    if (b & 3u) return fail(CQG_E_NONFINITE, "a trajectory produced a non-finite norm or rate");
+    if (b & 12u) return fail(CQG_E_STALLED, "a trajectory exhausted its step-size or attempt budget");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, double* run_ms) {
+  if (!ens) return fail(CQG_E_INVALID, "null argument");
+  if (kernel_ms) *kernel_ms = ens->lastMs;
+  if (run_ms) *run_ms = ens->lastRunMs;
+  return CQG_OK;
+}
+
+int cqg_probe_fma_peaks(double* fp64_tflops, double* fp32_tflops) {
+  return guardedCuda([&] {
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (fp64_tflops) *fp64_tflops = probe<double>(dev);
+    if (fp32_tflops) *fp32_tflops = probe<float>(dev);
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_destroy(cqg_ensemble* ens) {
+  delete ens;
+  return CQG_OK;
+}
+
+}  // extern "C"

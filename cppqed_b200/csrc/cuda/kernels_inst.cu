@@ -1,0 +1,28 @@
+// Explicit instantiation of the fused MCWF warp kernel for one (precision, rows per
+// lane) pair; the build compiles this file once per pair (-DCQG_REAL, -DCQG_E) so the
+// instances compile in parallel.  Exposes cqg_pick_<real>_e<E>(SMAX).
+#include "mcwf_kernel.cuh"
+
+#ifndef CQG_REAL
+#error "CQG_REAL must be defined"
+#endif
+#ifndef CQG_E
+#error "CQG_E must be defined"
+#endif
+
+#define CQG_CAT2(a, b, c) a##b##_e##c
+#define CQG_CAT(a, b, c) CQG_CAT2(a, b, c)
+
+namespace cqg {
+namespace dev {
+
+using KernelFn = void (*)(TrajDev, RunArgs);
+
+KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax) {
+  if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2>;
+  if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4>;
+  return &mcwfWarpKernel<CQG_REAL, CQG_E, 8>;
+}
+
+}  // namespace dev
+}  // namespace cqg

@@ -1,0 +1,708 @@
+// Fused MCWF trajectory kernel for sm_100a.
+//
+// One warp owns one trajectory at a time (persistent CTAs pull trajectories from a
+// device work queue).  Lane l owns state rows r = l + 32 e, e < E; the state, the
+// six Cash-Karp stage derivatives and the row's operator coefficients stay in
+// registers for the whole run.  The only cross-lane traffic is the banded H/i gather
+// (the stage vector is staged in a double-buffered shared-memory slab, one __syncwarp
+// per right-hand side) and the warp-shuffle reductions for the error norm, the norm,
+// the jump rates and the observables.  Everything the reference does per MCWF step
+// is fused here:
+//   ode_engine::Base::step + controlled Cash-Karp (ODE.h:234-262, Boost.Odeint)
+//   Exact::actWithU, renormalisation           (MCWF_Trajectory.h:250-276)
+//   rates, dpLimit control with step-back       (MCWF_Trajectory.h:279-317, 357-365)
+//   jump selection and J_m psi / sqrt(rate)     (MCWF_Trajectory.h:320-344)
+//   linear averages at every output time        (MCWF_Trajectory.h:406-420)
+#pragma once
+
+#include <cstdint>
+
+#include "rng.cuh"
+
+namespace cqg {
+namespace dev {
+
+constexpr int MAX_JUMPS = 8;
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---- complex helpers ---------------------------------------------------------
+template <typename R>
+struct CT;
+template <>
+struct CT<double> {
+  using T = double2;
+};
+template <>
+struct CT<float> {
+  using T = float2;
+};
+
+template <typename C2>
+__device__ __forceinline__ C2 mk(double x, double y) {
+  C2 r;
+  r.x = x;
+  r.y = y;
+  return r;
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 acc) {  // acc + a*b
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 acc) {
+  acc.x = fmaf(a.x, b.x, acc.x);
+  acc.x = fmaf(-a.y, b.y, acc.x);
+  acc.y = fmaf(a.x, b.y, acc.y);
+  acc.y = fmaf(a.y, b.x, acc.y);
+  return acc;
+}
+template <typename C2>
+__device__ __forceinline__ C2 cmul(C2 a, C2 b) {
+  C2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C2, typename S>
+__device__ __forceinline__ C2 axpy(S s, C2 v, C2 acc) {  // acc + s*v, s real
+  acc.x = fma(s, v.x, acc.x);
+  acc.y = fma(s, v.y, acc.y);
+  return acc;
+}
+template <typename C2>
+__device__ __forceinline__ double abs2(C2 a) {
+  return double(a.x) * double(a.x) + double(a.y) * double(a.y);
+}
+template <typename C2>
+__device__ __forceinline__ double cabs(C2 a) {
+  return hypot(double(a.x), double(a.y));
+}
+// exp(tau * f) for complex f, in double
+__device__ __forceinline__ double2 cexpScaled(double tau, double2 f) {
+  double s, c;
+  sincos(tau * f.y, &s, &c);
+  const double m = exp(tau * f.x);
+  return make_double2(m * c, m * s);
+}
+
+// ---- warp reductions -----------------------------------------------------------
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ double warpSum(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ double warpMax(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// ---- device-side system tables (see lowering.hpp) -----------------------------------
+struct SysDev {
+  int D, S, SJ, SO, nJ, nObs, nAvr;
+  int hasH, hasEx, hasFreq;
+  const int* col;        // [S][D]
+  const int* jcol;       // [nJ][SJ][D]
+  const double* jw;      // [nJ][D] rate weights
+  const int* jHasW;      // [nJ]
+  const int* ocol;       // [nObs][SO][D]
+  const double2* oval;   // [nObs][SO][D]
+  const int* oRe;        // [nObs]
+  const int* oIm;        // [nObs]
+  const double2* freq;   // [S][D] (IP) or null
+  const double2* lambda; // [D] (Exact) or null
+  // precision-specific copies
+  const double2* diagD;
+  const double2* valD;
+  const double2* jvalD;
+  const float2* diagF;
+  const float2* valF;
+  const float2* jvalF;
+};
+
+template <typename R>
+struct Tables;
+template <>
+struct Tables<double> {
+  __device__ static const double2* diag(const SysDev& s) { return s.diagD; }
+  __device__ static const double2* val(const SysDev& s) { return s.valD; }
+  __device__ static const double2* jval(const SysDev& s) { return s.jvalD; }
+};
+template <>
+struct Tables<float> {
+  __device__ static const float2* diag(const SysDev& s) { return s.diagF; }
+  __device__ static const float2* val(const SysDev& s) { return s.valF; }
+  __device__ static const float2* jval(const SysDev& s) { return s.jvalF; }
+};
+
+struct TrajDev {
+  int nTraj;
+  const int* sysIdx;
+  const SysDev* systems;
+  void* psi;                   // Real2 states
+  const long long* psiOff;     // element offset of each trajectory's state
+  double* t;
+  double* t0;
+  double* dtTry;
+  double* dtDid;
+  unsigned long long* rng;     // 4 words per trajectory
+  unsigned long long* cnt;     // 8 counters per trajectory
+  double* maxima;              // 3 per trajectory: dp overshoot, dp tolerance overshoot, |norm-1|
+  unsigned* status;
+  double* jumpT;               // [nTraj][jumpCap] ring
+  int* jumpL;
+  unsigned long long* jumpN;   // total jumps recorded per trajectory
+  int jumpCap;
+};
+
+enum RunMode { RUN_INTERVALS = 0, RUN_TO = 1, RUN_STEPS = 2 };
+
+struct RunArgs {
+  int mode;
+  double Dt;        // RUN_INTERVALS
+  int nIntervals;   // RUN_INTERVALS / RUN_STEPS
+  double tEnd;      // RUN_TO
+  int nSteps;       // RUN_STEPS: steps per interval
+  double T;         // RUN_STEPS: end time
+  double absSlot, relSlot;  // Odeint error-checker slots (eps_abs, eps_rel after the swap)
+  double dpLimit, overTol;
+  int maxAttempts;
+  int noise;
+  int rng;
+  unsigned long long seed;
+  long long maxStepsPerInterval;
+  unsigned long long timeLimitNs;  // wall-clock watchdog per trajectory task
+  double* avrOut;   // [nOut][nTraj][nAvrStride] or null
+  int nAvrStride;
+  int* queue;
+  const int* order;
+};
+
+// Cash-Karp tableau (published coefficients)
+struct CK {
+  static constexpr double c1 = 1. / 5, c2 = 3. / 10, c3 = 3. / 5, c4 = 1., c5 = 7. / 8;
+  static constexpr double a10 = 1. / 5;
+  static constexpr double a20 = 3. / 40, a21 = 9. / 40;
+  static constexpr double a30 = 3. / 10, a31 = -9. / 10, a32 = 6. / 5;
+  static constexpr double a40 = -11. / 54, a41 = 5. / 2, a42 = -70. / 27, a43 = 35. / 27;
+  static constexpr double a50 = 1631. / 55296, a51 = 175. / 512, a52 = 575. / 13824, a53 = 44275. / 110592,
+                          a54 = 253. / 4096;
+  static constexpr double b0 = 37. / 378, b2 = 250. / 621, b3 = 125. / 594, b5 = 512. / 1771;
+  static constexpr double e0 = 37. / 378 - 2825. / 27648, e2 = 250. / 621 - 18575. / 48384,
+                          e3 = 125. / 594 - 13525. / 55296, e4 = -277. / 14336, e5 = 512. / 1771 - 1. / 4;
+};
+
+template <typename R, int E, int SMAX>
+struct Worker {
+  using C2 = typename CT<R>::T;
+
+  const SysDev& sys;
+  const RunArgs& ra;
+  const int lane, D;
+  C2* buf0;
+  C2* buf1;
+  C2* cache;
+
+  // register-resident operator rows
+  C2 diag[E];
+  C2 val[E * SMAX <= 8 ? SMAX : 1][E];
+  int col[E * SMAX <= 8 ? SMAX : 1][E];
+
+  // state
+  C2 x[E];
+  double t, t0, dtTry, dtDid;
+  Pcg64 pcg;
+  unsigned long long draws;
+  unsigned long long ti;
+  unsigned long long nSteps, nAttempts, nFailed, nRhs, nOvershot, nBacks, nJumps;
+  double maxOvershoot, maxTolOvershoot, maxNormDev;
+  unsigned status;
+
+  __device__ Worker(const SysDev& s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c)
+      : sys(s), ra(a), lane(l), D(s.D), buf0(b0), buf1(b1), cache(c) {}
+
+  __device__ __forceinline__ int row(int e) const { return lane + 32 * e; }
+  __device__ __forceinline__ bool valid(int e) const { return row(e) < D; }
+
+  // Coefficients live in registers when E * SMAX is small (CREG), else they are
+  // re-read per right-hand side from global memory (L1-resident, shared by every
+  // trajectory of the system on the SM).
+  static constexpr bool CREG = E * SMAX <= 8;
+
+  __device__ void loadOperator() {
+    const C2* dg = Tables<R>::diag(sys);
+    const C2* vl = Tables<R>::val(sys);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int r = row(e);
+      const bool v = r < D;
+      diag[e] = v ? dg[r] : mk<C2>(0, 0);
+      if constexpr (CREG) {
+#pragma unroll
+        for (int s = 0; s < SMAX; ++s) {
+          const bool vs = v && s < sys.S;
+          col[s][e] = vs ? sys.col[s * D + r] : 0;
+          val[s][e] = vs ? vl[s * D + r] : mk<C2>(0, 0);
+        }
+      }
+    }
+  }
+
+  // out = (H/i) y at picture time tau; y staged through `buf`
+  __device__ __forceinline__ void rhs(const C2 (&y)[E], C2 (&out)[E], double tau, C2* buf) {
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (valid(e)) buf[row(e)] = y[e];
+    __syncwarp();
+    ++nRhs;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      C2 acc = cmul(diag[e], y[e]);
+      const int r = valid(e) ? row(e) : 0;
+#pragma unroll
+      for (int s = 0; s < SMAX; ++s) {
+        if (s < sys.S) {
+          C2 c;
+          int cc;
+          if constexpr (CREG) {
+            c = val[s][e];
+            cc = col[s][e];
+          } else {
+            c = valid(e) ? __ldg(&Tables<R>::val(sys)[s * D + r]) : mk<C2>(0, 0);
+            cc = __ldg(&sys.col[s * D + r]);
+          }
+          if (sys.hasFreq && valid(e)) {
+            const double2 f = sys.freq[s * D + r];
+            if (f.x != 0. || f.y != 0.) {
+              const double2 ph = cexpScaled(tau, f);
+              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+            }
+          }
+          acc = cfma(c, buf[cc], acc);
+        }
+      }
+      out[e] = acc;
+    }
+  }
+
+  // one adaptive ODE step towards at most deltaT (ode_engine::Base::step)
+  __device__ bool odeStep(double deltaT) {
+    const double timeBefore = t;
+    const double nextDtTry = fabs(deltaT) < fabs(dtTry / 10.) ? dtTry : 0.;
+    if (fabs(dtTry) > fabs(deltaT)) dtTry = deltaT;
+    C2 k0[E], k1[E], k2[E], k3[E], k4[E], k5[E], y[E];
+    rhs(x, k0, t - t0, buf0);
+    for (int attempt = 0;; ++attempt) {
+      if (attempt >= ra.maxAttempts) {
+        status |= 8u;  // CQG_TRAJ_ATTEMPT_LIMIT
+        return false;
+      }
+      ++nAttempts;
+      const double dt = dtTry;
+      const R s10 = R(dt * CK::a10);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s10, k0[e], x[e]);
+      rhs(y, k1, t + CK::c1 * dt - t0, buf1);
+      {
+        const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
+#pragma unroll
+        for (int e = 0; e < E; ++e) y[e] = axpy(s1, k1[e], axpy(s0, k0[e], x[e]));
+      }
+      rhs(y, k2, t + CK::c2 * dt - t0, buf0);
+      {
+        const R s0 = R(dt * CK::a30), s1 = R(dt * CK::a31), s2 = R(dt * CK::a32);
+#pragma unroll
+        for (int e = 0; e < E; ++e) y[e] = axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])));
+      }
+      rhs(y, k3, t + CK::c3 * dt - t0, buf1);
+      {
+        const R s0 = R(dt * CK::a40), s1 = R(dt * CK::a41), s2 = R(dt * CK::a42), s3 = R(dt * CK::a43);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          y[e] = axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e]))));
+      }
+      rhs(y, k4, t + CK::c4 * dt - t0, buf0);
+      {
+        const R s0 = R(dt * CK::a50), s1 = R(dt * CK::a51), s2 = R(dt * CK::a52), s3 = R(dt * CK::a53),
+                s4 = R(dt * CK::a54);
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          y[e] = axpy(s4, k4[e], axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])))));
+      }
+      rhs(y, k5, t + CK::c5 * dt - t0, buf1);
+      // 5th-order solution, embedded error and the Odeint error norm
+      const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
+      const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4), e5 = R(dt * CK::e5);
+      const double adt = fabs(dt);
+      double errLocal = 0.;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        y[e] = axpy(b5, k5[e], axpy(b3, k3[e], axpy(b2, k2[e], axpy(b0, k0[e], x[e]))));
+        C2 xe = mk<C2>(0, 0);
+        xe = axpy(e5, k5[e], axpy(e4, k4[e], axpy(e3, k3[e], axpy(e2, k2[e], axpy(e0, k0[e], xe)))));
+        if (valid(e)) {
+          const double den = ra.absSlot + ra.relSlot * (cabs(x[e]) + adt * cabs(k0[e]));
+          errLocal = fmax(errLocal, cabs(xe) / den);
+        }
+      }
+      double err = warpMax(errLocal);
+      if (!(err == err)) {  // NaN error norm
+        status |= 1u;
+        return false;
+      }
+      if (err > 1.0) {
+        dtTry = dt * fmax(0.9 * pow(err, -1. / 3.), 0.2);
+        ++nFailed;
+        if (!(dtTry > 0.) || t + dtTry == t) {
+          status |= 4u;  // CQG_TRAJ_DT_UNDERFLOW
+          return false;
+        }
+        __syncwarp();  // the retry rewrites the buffer the last stage read
+        continue;
+      }
+      t += dt;
+      if (err < 0.5) {
+        err = fmax(3.2e-4, err);  // 5^-5
+        dtTry = dt * 0.9 * pow(err, -1. / 5.);
+      } else
+        dtTry = dt;
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = y[e];
+      break;
+    }
+    dtDid = t - timeBefore;
+    if (nextDtTry != 0.) dtTry = nextDtTry;
+    return true;
+  }
+
+  __device__ bool coherentTimeDevelopment(double Dt, bool li) {
+    if (sys.hasH) {
+      if (!odeStep(Dt)) return false;
+    } else {
+      const double stepToDo = li ? fmin(dtTry, Dt) : Dt;
+      t += stepToDo;
+      dtDid = stepToDo;
+    }
+    if (sys.hasEx) {
+      const double tau = t - t0;
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (valid(e)) {
+          const double2 u = cexpScaled(tau, sys.lambda[row(e)]);
+          x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
+        }
+      t0 = t;
+    }
+    double n2 = 0.;
+#pragma unroll
+    for (int e = 0; e < E; ++e) n2 += abs2(x[e]);
+    n2 = warpSum(n2);
+    const double n = sqrt(n2);
+    if (!(n > 0.) || !isfinite(n)) {
+      status |= 1u;  // CQG_TRAJ_NONFINITE_NORM
+      return false;
+    }
+    const double inv = 1. / n;
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(x[e].x) * inv, double(x[e].y) * inv);
+    maxNormDev = fmax(maxNormDev, fabs(1. - n));
+    return true;
+  }
+
+  // (J_m psi) rows into out; psi staged in buf (caller synchronised)
+  __device__ __forceinline__ void applyJump(int m, const C2* buf, C2 (&out)[E]) const {
+    const C2* jv = Tables<R>::jval(sys) + size_t(m) * sys.SJ * D;
+    const int* jc = sys.jcol + size_t(m) * sys.SJ * D;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      C2 acc = mk<C2>(0, 0);
+      if (valid(e))
+        for (int s = 0; s < sys.SJ; ++s) acc = cfma(jv[s * D + row(e)], buf[jc[s * D + row(e)]], acc);
+      out[e] = acc;
+    }
+  }
+
+  __device__ bool computeRates(double (&rates)[MAX_JUMPS]) {
+    double part[MAX_JUMPS];
+    bool anySpecial = false;
+    for (int m = 0; m < sys.nJ; ++m) anySpecial |= !sys.jHasW[m];
+    if (anySpecial) {
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (valid(e)) buf0[row(e)] = x[e];
+      __syncwarp();
+    }
+    for (int m = 0; m < sys.nJ; ++m) {
+      double acc = 0.;
+      if (sys.jHasW[m]) {
+        const double* w = sys.jw + size_t(m) * D;
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (valid(e)) acc += w[row(e)] * abs2(x[e]);
+      } else {
+        C2 jx[E];
+        applyJump(m, buf0, jx);
+#pragma unroll
+        for (int e = 0; e < E; ++e) acc += abs2(jx[e]);
+      }
+      part[m] = acc;
+    }
+    if (anySpecial) __syncwarp();
+    bool ok = true;
+    for (int m = 0; m < sys.nJ; ++m) {
+      rates[m] = warpSum(part[m]);
+      ok &= isfinite(rates[m]);
+    }
+    if (!ok) status |= 2u;  // CQG_TRAJ_NONFINITE_RATE
+    return ok;
+  }
+
+  // MCWF_Trajectory::manageTimeStep; true = step back
+  __device__ bool manageTimeStep(const double (&rates)[MAX_JUMPS], double tCache, double dtDidCache) {
+    double totalRate = 0.;
+    for (int m = 0; m < sys.nJ; ++m) totalRate += rates[m];
+    const double liouvilleanSuggestedDtTry = ra.dpLimit / totalRate;
+    if (totalRate * dtDid > ra.overTol * ra.dpLimit) {
+      maxTolOvershoot = fmax(maxTolOvershoot, totalRate * dtDid);
+      t = tCache;
+      dtDid = dtDidCache;
+      dtTry = liouvilleanSuggestedDtTry;
+      ++nBacks;
+      return true;
+    } else if (totalRate * dtTry > ra.dpLimit) {
+      ++nOvershot;
+      maxOvershoot = fmax(maxOvershoot, totalRate * dtTry);
+    }
+    dtTry = sys.hasH ? fmin(dtTry, liouvilleanSuggestedDtTry) : liouvilleanSuggestedDtTry;
+    return false;
+  }
+
+  __device__ double uniform() {
+    double u = 0.;
+    if (lane == 0) {
+      if (ra.rng == 0)
+        u = canonicalFromU64(pcg.next());
+      else
+        u = philoxUniform(ra.seed, ti, draws);
+    }
+    ++draws;
+    return __shfl_sync(FULL, u, 0);
+  }
+
+  __device__ bool performJump(const double (&rates)[MAX_JUMPS], const TrajDev& td) {
+    double random = uniform() / dtDid;
+    int lindbladNo = 0;
+    for (; random > 0 && lindbladNo != sys.nJ; random -= rates[lindbladNo++])
+      ;
+    if (random < 0) {
+      --lindbladNo;
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (valid(e)) buf0[row(e)] = x[e];
+      __syncwarp();
+      C2 jx[E];
+      applyJump(lindbladNo, buf0, jx);
+      __syncwarp();
+      const double normFactor = sqrt(rates[lindbladNo]);
+      if (!isfinite(normFactor) || !(normFactor > 0.)) {
+        status |= 1u;
+        return false;
+      }
+      const double inv = 1. / normFactor;
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(jx[e].x) * inv, double(jx[e].y) * inv);
+      if (lane == 0 && td.jumpCap > 0) {
+        const unsigned long long slot = nJumps % (unsigned long long)td.jumpCap;
+        td.jumpT[ti * td.jumpCap + slot] = t;
+        td.jumpL[ti * td.jumpCap + slot] = lindbladNo;
+      }
+      ++nJumps;
+    }
+    return true;
+  }
+
+  // MCWF_Trajectory::step
+  __device__ bool step(double Dt, const TrajDev& td) {
+    const bool li = ra.noise && sys.nJ > 0;
+    const double tCache = t, dtDidCache = dtDid;
+    if (li) {
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (valid(e)) cache[row(e)] = x[e];
+    }
+    if (!coherentTimeDevelopment(Dt, li)) return false;
+    if (li) {
+      double rates[MAX_JUMPS];
+      if (!computeRates(rates)) return false;
+      int backs = 0;
+      while (manageTimeStep(rates, tCache, dtDidCache)) {
+        if (++backs > 10000) {
+          status |= 8u;
+          return false;
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (valid(e)) x[e] = cache[row(e)];
+        if (!coherentTimeDevelopment(Dt, li)) return false;
+        if (!computeRates(rates)) return false;
+      }
+      if (!performJump(rates, td)) return false;
+    }
+    ++nSteps;
+    return true;
+  }
+
+  // per-trajectory linear averages <psi|O_k|psi>
+  __device__ void averages(double* out) {
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (valid(e)) buf0[row(e)] = x[e];
+    __syncwarp();
+    for (int k = 0; k < sys.nObs; ++k) {
+      const double2* ov = sys.oval + size_t(k) * sys.SO * D;
+      const int* oc = sys.ocol + size_t(k) * sys.SO * D;
+      double re = 0., im = 0.;
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (valid(e)) {
+          double2 acc = make_double2(0., 0.);
+          for (int s = 0; s < sys.SO; ++s) {
+            const C2 v = buf0[oc[s * D + row(e)]];
+            acc = cfma(ov[s * D + row(e)], make_double2(double(v.x), double(v.y)), acc);
+          }
+          const double xr = double(x[e].x), xi = double(x[e].y);
+          re += xr * acc.x + xi * acc.y;  // conj(x) * acc
+          im += xr * acc.y - xi * acc.x;
+        }
+      re = warpSum(re);
+      im = warpSum(im);
+      if (lane == 0 && out) {
+        if (sys.oRe[k] >= 0) out[sys.oRe[k]] = re;
+        if (sys.oIm[k] >= 0) out[sys.oIm[k]] = im;
+      }
+    }
+    __syncwarp();
+  }
+
+  __device__ void run(const TrajDev& td, int trajIndex) {
+    ti = (unsigned long long)trajIndex;
+    C2* psi = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
+    loadOperator();
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = valid(e) ? psi[row(e)] : mk<C2>(0, 0);
+    t = td.t[ti];
+    t0 = td.t0[ti];
+    dtTry = td.dtTry[ti];
+    dtDid = td.dtDid[ti];
+    const unsigned long long* rs = td.rng + 4 * ti;
+    pcg.state.hi = rs[0];
+    pcg.state.lo = rs[1];
+    pcg.inc.hi = rs[2];
+    pcg.inc.lo = rs[3];
+    draws = rs[0];  // philox keeps its draw counter in word 0
+    const unsigned long long* c = td.cnt + 8 * ti;
+    nSteps = c[0];
+    nAttempts = c[1];
+    nFailed = c[2];
+    nRhs = c[3];
+    nOvershot = c[4];
+    nBacks = c[5];
+    nJumps = c[6];
+    maxOvershoot = td.maxima[3 * ti];
+    maxTolOvershoot = td.maxima[3 * ti + 1];
+    maxNormDev = td.maxima[3 * ti + 2];
+    status = td.status[ti];
+
+    const int nOut = ra.mode == RUN_TO ? 1 : ra.nIntervals;
+    const unsigned long long tStart = globalTimerNs();
+    for (int k = 0; k < nOut && status == 0u; ++k) {
+      long long guard = 0;
+      if (ra.mode == RUN_STEPS) {
+        for (int s = 0; s < ra.nSteps && t < ra.T; ++s)
+          if (!step(ra.T - t, td)) break;
+      } else {
+        const double endTime = ra.mode == RUN_TO ? ra.tEnd : t + ra.Dt;
+        double dt;
+        while ((dt = endTime - t) != 0.) {
+          // bounded: a negative remainder, a step budget, or the wall-clock watchdog
+          // end the trajectory with an error status instead of spinning
+          if (dt < 0. || ++guard > ra.maxStepsPerInterval ||
+              ((guard & 63) == 0 && globalTimerNs() - tStart > ra.timeLimitNs)) {
+            status |= 8u;
+            break;
+          }
+          if (!step(dt, td)) break;
+        }
+      }
+      if (ra.avrOut) {
+        double* slot = ra.avrOut + ((size_t)k * td.nTraj + ti) * ra.nAvrStride;
+        averages(slot);
+        if (lane == 0) slot[ra.nAvrStride - 1] = dtDid;
+      }
+    }
+
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (valid(e)) psi[row(e)] = x[e];
+    if (lane == 0) {
+      td.t[ti] = t;
+      td.t0[ti] = t0;
+      td.dtTry[ti] = dtTry;
+      td.dtDid[ti] = dtDid;
+      unsigned long long* rw = td.rng + 4 * ti;
+      if (ra.rng == 0) {
+        rw[0] = pcg.state.hi;
+        rw[1] = pcg.state.lo;
+        rw[2] = pcg.inc.hi;
+        rw[3] = pcg.inc.lo;
+      } else {
+        rw[0] = draws;
+      }
+      unsigned long long* cw = td.cnt + 8 * ti;
+      cw[0] = nSteps;
+      cw[1] = nAttempts;
+      cw[2] = nFailed;
+      cw[3] = nRhs;
+      cw[4] = nOvershot;
+      cw[5] = nBacks;
+      cw[6] = nJumps;
+      cw[7] = status;
+      td.maxima[3 * ti] = maxOvershoot;
+      td.maxima[3 * ti + 1] = maxTolOvershoot;
+      td.maxima[3 * ti + 2] = maxNormDev;
+      td.status[ti] = status;
+      if (td.jumpN) td.jumpN[ti] = nJumps;
+    }
+  }
+};
+
+template <typename R, int E, int SMAX>
+__global__ void __launch_bounds__(128) mcwfWarpKernel(TrajDev td, RunArgs ra) {
+  using C2 = typename CT<R>::T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int DMAX = 32 * E;
+  C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * 3 * DMAX;
+  while (true) {
+    int task = 0;
+    if (lane == 0) task = atomicAdd(ra.queue, 1);
+    task = __shfl_sync(FULL, task, 0);
+    if (task >= td.nTraj) return;
+    const int ti = ra.order ? ra.order[task] : task;
+    const SysDev& sys = td.systems[td.sysIdx[ti]];
+    Worker<R, E, SMAX> w(sys, ra, lane, base, base + DMAX, base + 2 * DMAX);
+    w.run(td, ti);
+    __syncwarp();
+  }
+}
+
+}  // namespace dev
+}  // namespace cqg

@@ -171,23 +171,25 @@ int cqg_batch_create(const cqg_system* const* systems, int32_t n_systems, const 
 
 /* Advance every trajectory by exactly Dt, n_intervals times (cppqedutils::advance,
  * Trajectory.h:44-50, inside Ensemble::advance, StochasticTrajectory.h:220).
- * After interval k the ensemble-summed linear averages are written to
- * avr_out[k*n_avr + c] (host pointer, may be NULL) — divide by n_traj for the
- * ensemble mean; the reference streams (1/N) Tr(rho O), MCWF_Trajectory.h:406-420.
- * In batch mode each trajectory's own averages are kept per system; use
- * cqg_ensemble_traj_averages for them.                                     */
+ * After interval k the ensemble sums are written to avr_out[k*(n_avr+1) + c]
+ * (host pointer, may be NULL): columns 0..n_avr-1 the linear averages, column
+ * n_avr the dtDid — divide by n_traj for the ensemble mean; the reference streams
+ * (1/N) Tr(rho O) and the mean dtDid (MCWF_Trajectory.h:406-420,
+ * StochasticTrajectory.h:223-226).  In batch mode the columns of systems with
+ * different observables are mixed; use cqg_ensemble_traj_averages instead.  */
 int cqg_ensemble_run(cqg_ensemble* ens, double Dt, int32_t n_intervals, double* avr_out);
 
 /* Same as cqg_ensemble_run but every trajectory advances to the absolute
  * time t_end (used for the T-capped final interval in Dt mode). */
 int cqg_ensemble_advance_to(cqg_ensemble* ens, double t_end, double* avr_out);
 
-/* Single trajectory: `n_steps` MCWF steps, each MCWF_Trajectory::step(T - t)
- * (the dc-mode loop of trajectory::run, Trajectory.h:560-595), stopping early
- * at T.  Applies to every trajectory of the ensemble. */
+/* `n_steps` MCWF steps per trajectory, each MCWF_Trajectory::step(T - t) (the
+ * dc-mode loop of trajectory::run, Trajectory.h:560-595), stopping early at T.
+ * n_steps = 0 only evaluates the averages of the current states. */
 int cqg_ensemble_steps(cqg_ensemble* ens, int32_t n_steps, double T, double* avr_out);
 
-/* Per-trajectory linear averages at the current time: out[i*n_avr + c]. */
+/* Per-trajectory averages of the first output of the last run call:
+ * out[i*(n_avr+1) + c], column n_avr = dtDid. */
 int cqg_ensemble_traj_averages(cqg_ensemble* ens, double* out);
 
 int cqg_ensemble_size(const cqg_ensemble* ens, int64_t* n_traj, int32_t* n_avr);
@@ -213,8 +215,15 @@ int cqg_ensemble_get_jumps(const cqg_ensemble* ens, int64_t i, int32_t cap, doub
 /* OR of all trajectory status bits; CQG_E_NONFINITE / CQG_E_STALLED when set. */
 int cqg_ensemble_status(const cqg_ensemble* ens, uint32_t* bits);
 
-/* Device time of the last run call in milliseconds (CUDA events). */
-int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* ms);
+/* Device times of the last run call in milliseconds (CUDA events on the
+ * ensemble's stream): the MCWF kernel alone, and every device operation of the
+ * call (initialisation, kernel, reduction, read-back).  Either pointer may be NULL. */
+int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, double* run_ms);
+
+/* Measured FMA throughput of the current device (TFLOP/s, 2 flops per FMA) for
+ * FP64 and FP32 CUDA cores: the denominator of the kernels' roofline and an
+ * input of the launch-shape tuner.  Runs two short probe kernels. */
+int cqg_probe_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 
 int cqg_ensemble_destroy(cqg_ensemble* ens);
 

@@ -1,0 +1,63 @@
+"""Extracts the numeric columns of the reference's golden runs into JSON fixtures.
+
+Reads Testing/expected/run_<name> (C++QED v2.120, written by CPPQEDscripts with the
+command lines of Testing/run/testdriver.conf) and stores, per run, the command line,
+the streamed rows (time, dtDid, averages) and the pcg64 engine state serialised in
+the first archive of the matching .state file (the engine right after seeding).
+Run once where the reference tree is available:
+
+    python tests/golden/make_golden.py /path/to/reference
+"""
+import bz2
+import json
+import os
+import re
+import sys
+
+RUNS = ["run_PTLA_CPPQED_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
+RUNS += ["run_1particle1mode_%s_%s" % (m, e) for m in ("dc", "dt", "ndt", "ndt_conf2", "ndt_conf3", "ndt_conf4")
+         for e in ("single", "ensemble", "master")]
+RUNS += ["run_Ring_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
+
+
+def parse(path):
+    cmd, rows = None, []
+    for line in open(path):
+        if line.startswith("#"):
+            if cmd is None and line.strip() != "#":
+                cmd = line[1:].strip()
+            continue
+        if line.strip():
+            rows.append([float(x) for x in line.split()])
+    return cmd, rows
+
+
+def pcg_state(path):
+    if not os.path.exists(path):
+        return None
+    raw = bz2.decompress(open(path, "rb").read())
+    m = re.search(rb"(\d{20,}) (\d+) (\d{10,}) ", raw)
+    return m.group(0).decode().strip() if m else None
+
+
+def main(ref):
+    exp = os.path.join(ref, "Testing", "expected")
+    out = {}
+    for r in RUNS:
+        p = os.path.join(exp, r)
+        if not os.path.exists(p):
+            continue
+        cmd, rows = parse(p)
+        args = cmd.split()[1:]
+        if "--o" in args:
+            i = args.index("--o")
+            del args[i:i + 2]
+        out[r] = {"script": os.path.basename(cmd.split()[0]), "args": args, "rows": rows,
+                  "pcg64_first_archive": pcg_state(p + ".state")}
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_runs.json")
+    json.dump(out, open(dst, "w"), indent=0)
+    print("wrote", dst, len(out), "runs")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

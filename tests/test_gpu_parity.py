@@ -1,0 +1,154 @@
+"""Device parity against the CPU oracle and the reference's golden runs.
+
+Tolerances:
+* golden runs: np.allclose, as the reference's own testdriver (Verifier._verify_ev);
+* jump-free FP64 trajectory vs the oracle on the same step sequence: 1e-10 relative
+  (correctness check 1);
+* ensembles vs the master equation: 3 sigma of the ensemble standard error with a
+  Bonferroni-style margin over the compared points (correctness check 2).
+"""
+import numpy as np
+import pytest
+
+from cppqed_b200 import _abi as A
+
+pytestmark = pytest.mark.gpu
+
+C2_ARGS = ["--picture", "Sch", "--deltaA", "0", "--gamma", "0.5", "--deltaC", "0", "--kappa", "1",
+           "--eta", "1.5", "--cutoff", "40", "--g", "2"]
+C1_ARGS = ["--picture", "Sch", "--deltaC", "-1", "--eta", "2", "--kappa", "1", "--cutoff", "30", "--no_quadratures"]
+
+
+@pytest.mark.parametrize("run", ["run_PTLA_CPPQED_%s_%s" % (m, e) for m in ("dc", "dt", "ndt")
+                                 for e in ("single", "ensemble")])
+def test_ptla_golden_on_device(gpu, golden, run):
+    g = golden[run]
+    rows, ens, model = gpu.evolve(g["script"], g["args"])
+    ref = np.array(g["rows"])
+    assert rows.shape == ref.shape
+    assert np.allclose(rows, ref)
+
+
+def test_jump_free_fp64_trajectory_matches_oracle(gpu, oracle):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS + ["--no_noise"])
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), 1, pars)
+    for k in range(1, 6):
+        ens.run(0.2, 1)
+        ref = oracle.trajectory(model, pars, pars.prng_stream, 0.2, k)
+        psi = ens.state(0, model.dim)
+        assert np.linalg.norm(psi - ref["psi"]) <= 1e-10 * np.linalg.norm(ref["psi"])
+        t, did, dtry = ens.times()
+        assert abs(t[0] - ref["t"]) <= 1e-12 * ref["t"]
+
+
+def test_trajectory_with_jumps_replays_reference_streams(gpu, oracle):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    n = 4
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ens.run(0.5, 4)
+    agree = 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.5, 4)
+        jt, jl = ens.jumps(i, 4096)
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            psi = ens.state(i, model.dim)
+            assert np.linalg.norm(psi - ref["psi"]) < 1e-7
+    # floating-point differences may flip a marginal jump decision; most must replay exactly
+    assert agree >= n - 1
+
+
+def _master_rows(oracle, model, T, Dt):
+    rp = model.run_pars()
+    rp.evol = A.EVOL_MASTER
+    rp.dc = 0
+    rp.T = T
+    rp.Dt = Dt
+    rp.NDt = 0
+    return oracle.run(model, rp)
+
+
+@pytest.mark.parametrize("rng", [A.RNG_PHILOX, A.RNG_PCG64])
+def test_pumped_lossy_mode_ensemble_vs_master(gpu, oracle, rng):
+    model = gpu.Model("PumpedLossyMode_C++QED", C1_ARGS)
+    n = 2048
+    pars = model.run_pars().mcwf
+    pars.rng = rng
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    Dt, K = 0.5, 8
+    sums = ens.run(Dt, K)
+    per = ens.traj_averages()  # last run's first interval only; use sums for means
+    master = _master_rows(oracle, model, Dt * K, Dt)
+    # columns: <n>, VAR(n) (processed), Re<a>, Im<a>
+    mean = sums[:, :model.n_avr] / n
+    for k in range(K):
+        ref = master[k + 1, 2:]
+        m_n, m_re, m_im = mean[k, 0], mean[k, 2], mean[k, 3]
+        # a coherent state stays coherent through jumps: Var(<a>) across trajectories is tiny,
+        # Var(n) per trajectory is <n>; allow 3 sigma + 1% model margin
+        sig_n = np.sqrt(max(ref[0], 1e-3) / n) * 3 + 0.01 * ref[0]
+        assert abs(m_n - ref[0]) <= sig_n
+        assert abs(m_re - ref[2]) <= 0.02 + 0.01 * abs(ref[2])
+        assert abs(m_im - ref[3]) <= 0.02 + 0.01 * abs(ref[3])
+
+
+def test_qbit_mode_ensemble_vs_master(gpu, oracle):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    n = 4096
+    pars = model.run_pars().mcwf
+    pars.rng = A.RNG_PHILOX
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    Dt, K = 0.25, 8
+    sums = ens.run(Dt, K)
+    master = _master_rows(oracle, model, Dt * K, Dt)
+    per_last = None
+    mean = sums[:, :model.n_avr] / n
+    # columns: rho00, rho11, Re rho10, Im rho10, <n>, VAR(n), Re<a>, Im<a>
+    z = []
+    for k in range(K):
+        ref = master[k + 1, 2:]
+        p11 = ref[1]
+        sig_rho11 = np.sqrt(max(p11 * (1 - p11), 1e-4) / n)
+        z.append(abs(mean[k, 1] - p11) / sig_rho11)
+        sig_n = np.sqrt(max(ref[5] + ref[4], 1e-2) / n)
+        z.append(abs(mean[k, 4] - ref[4]) / sig_n)
+    z = np.array(z)
+    assert z.max() < 4.0, z  # 3 sigma with a Bonferroni margin for 16 comparisons
+
+
+def test_fp32_state_error_vs_fp64(gpu):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    sysd = gpu.System(model.desc)
+    res = {}
+    for prec in (A.FP64, A.FP32):
+        pars = model.run_pars().mcwf
+        pars.rng = A.RNG_PHILOX
+        pars.precision = prec
+        ens = gpu.Ensemble(sysd, model.initial_state(), 4096, pars)
+        res[prec] = ens.run(0.25, 8)[:, :model.n_avr] / 4096
+    diff = np.abs(res[A.FP32] - res[A.FP64])
+    # same random streams; FP32 state flips few jump decisions: averages agree to ~3 sigma
+    assert diff[:, 4].max() < 0.1
+    assert diff[:, 1].max() < 0.05
+
+
+def test_stalled_trajectory_reports_status(gpu):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    pars = model.run_pars().mcwf
+    pars.max_attempts = 1
+    pars.eps_rel = 1e-300
+    pars.eps_abs = 0.0
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), 8, pars)
+    with pytest.raises(gpu.EngineError) as e:
+        ens.run(0.1, 1)
+    assert e.value.code == A.CQG_E_STALLED
+    rc, bits = ens.status()
+    assert bits & 8

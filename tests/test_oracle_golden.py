@@ -1,0 +1,45 @@
+"""The CPU oracle against the reference's own golden runs (Testing/expected, as
+fixtures in tests/golden/reference_runs.json).  These pin the oracle: the Odeint
+controller with its swapped eps arguments, the MCWF step, pcg64 streams, the run
+loops, the ensemble density-operator average and the master equation."""
+import numpy as np
+import pytest
+
+from cppqed_b200 import _abi as A
+
+PTLA = ["run_PTLA_CPPQED_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
+
+
+@pytest.mark.parametrize("run", PTLA)
+def test_ptla_golden(engine, oracle, golden, run):
+    g = golden[run]
+    model = engine.Model(g["script"], g["args"])
+    rows = oracle.run(model)
+    ref = np.array(g["rows"])
+    assert rows.shape == ref.shape
+    # testdriver.py Verifier._verify_ev: np.allclose on all streamed columns
+    assert np.allclose(rows, ref)
+
+
+def test_pcg64_seeding_matches_reference_archive(oracle, golden):
+    # the first state archive of a single run holds the engine right after pcg64{1001, 1}
+    state = golden["run_PTLA_CPPQED_dc_single"]["pcg64_first_archive"]
+    assert oracle.pcg64_state_text(1001, 1) == state
+
+
+def test_eps_arguments_are_swapped_as_in_the_reference(engine, oracle, golden):
+    # make_controlled(epsRel, epsAbs, ...) puts epsRel into Odeint's absolute slot
+    # (ODE.h:205); with the slots the other way round the dtDid column differs.
+    g = golden["run_PTLA_CPPQED_dc_single"]
+    model = engine.Model(g["script"], g["args"])
+    rp = model.run_pars()
+    rp.mcwf.eps_rel, rp.mcwf.eps_abs = rp.mcwf.eps_abs, rp.mcwf.eps_rel
+    rows = oracle.run(model, rp)
+    ref = np.array(g["rows"])
+    assert rows.shape != ref.shape or not np.allclose(rows, ref)
+
+
+def test_uniform_draws_are_canonical(oracle):
+    u = oracle.pcg64_uniform(1001, 1, 10000)
+    assert u.min() >= 0 and u.max() < 1
+    assert abs(u.mean() - 0.5) < 0.02
