@@ -243,8 +243,10 @@ namespace cqg {
 namespace dev {
 KernelFn pick_double_e1(int smax);
 KernelFn pick_double_e2(int smax);
+KernelFn pick_double_e3(int smax);
 KernelFn pick_double_e4(int smax);
 KernelFn pick_float_e1(int smax);
+KernelFn pick_float_e3(int smax);
 KernelFn pick_float_e2(int smax);
 KernelFn pick_float_e4(int smax);
 }  // namespace dev
@@ -253,8 +255,15 @@ KernelFn pick_float_e4(int smax);
 namespace {
 
 KernelFn pickKernel(bool fp64, int E, int SMAX) {
-  if (fp64) return E == 1 ? dev::pick_double_e1(SMAX) : E == 2 ? dev::pick_double_e2(SMAX) : dev::pick_double_e4(SMAX);
-  return E == 1 ? dev::pick_float_e1(SMAX) : E == 2 ? dev::pick_float_e2(SMAX) : dev::pick_float_e4(SMAX);
+  if (fp64)
+    return E == 1 ? dev::pick_double_e1(SMAX)
+         : E == 2 ? dev::pick_double_e2(SMAX)
+         : E == 3 ? dev::pick_double_e3(SMAX)
+                  : dev::pick_double_e4(SMAX);
+  return E == 1 ? dev::pick_float_e1(SMAX)
+       : E == 2 ? dev::pick_float_e2(SMAX)
+       : E == 3 ? dev::pick_float_e3(SMAX)
+                : dev::pick_float_e4(SMAX);
 }
 
 __global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, int nAvrStride, int nAvr,
@@ -457,11 +466,12 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   ra.maxStepsPerInterval = 2000000000LL;
   ra.timeLimitNs = 120ull * 1000000000ull;
 
-  const int E = e->Dmax <= 32 ? 1 : e->Dmax <= 64 ? 2 : 4;
+  const int E = (e->Dmax + 31) / 32;  // rows per lane, 1..4
   const int SM = e->Smax <= 2 ? 2 : e->Smax <= 4 ? 4 : 8;
   KernelFn fn = pickKernel(e->pars.precision == CQG_FP64, E, SM);
   const int threads = 128;
-  const size_t smem = size_t(threads / 32) * 3 * 32 * E * e->elemBytes;
+  const size_t smem =
+      size_t(threads / 32) * 3 * 32 * E * e->elemBytes + size_t(threads / 32) * sizeof(dev::WarpScratch);
   ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
      "cudaFuncSetAttribute");
   int perSM = 0, nSM = 0;

@@ -77,10 +77,11 @@ __device__ __forceinline__ double abs2(C2 a) {
 }
 template <typename C2>
 __device__ __forceinline__ double cabs(C2 a) {
-  return hypot(double(a.x), double(a.y));
+  return sqrt(double(a.x) * double(a.x) + double(a.y) * double(a.y));
 }
-// exp(tau * f) for complex f, in double
-__device__ __forceinline__ double2 cexpScaled(double tau, double2 f) {
+// exp(tau * f) for complex f, in double.  Kept out of line: sincos/exp expand to a lot
+// of code and are only needed in the interaction picture.
+static __device__ __noinline__ double2 cexpScaled(double tau, double2 f) {
   double s, c;
   sincos(tau * f.y, &s, &c);
   const double m = exp(tau * f.x);
@@ -99,6 +100,27 @@ __device__ __forceinline__ double warpSum(double v) {
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
   return v;
 }
+// sums of n <= N warp-uniform values at once (independent shuffles pipeline)
+template <int N>
+__device__ __forceinline__ void warpSumN(double (&v)[N], int n) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+      if (m < n) v[m] += __shfl_xor_sync(FULL, v[m], o);
+  }
+}
+
+// Odeint's default step adjuster (decrease: max(0.9 err^(-1/(error order - 1)), 0.2);
+// increase below err 0.5: 0.9 max(err, 5^-5)^(-1/stepper order)), out of line for code size.
+static __device__ __noinline__ double decreasedStep(double dt, double err) {
+  return dt * fmax(0.9 * pow(err, -1. / 3.), 0.2);
+}
+static __device__ __noinline__ double increasedStep(double dt, double err) {
+  err = fmax(3.2e-4, err);  // 5^-5
+  return dt * 0.9 * pow(err, -1. / 5.);
+}
+
 __device__ __forceinline__ double warpMax(double v) {
 #pragma unroll
   for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
@@ -200,46 +222,67 @@ struct CK {
                           e3 = 125. / 594 - 13525. / 55296, e4 = -277. / 14336, e5 = 512. / 1771 - 1. / 4;
 };
 
+// Per-warp shared scratch next to the state slabs.
+struct WarpScratch {
+  unsigned long long pcg[4];  // state hi, lo, increment hi, lo (pcg64); word 0 = draw count (philox)
+};
+
 template <typename R, int E, int SMAX>
 struct Worker {
   using C2 = typename CT<R>::T;
 
-  const SysDev& sys;
+  // hot system fields in registers; the rest is read through sysp on rare paths
+  const SysDev* sysp;
   const RunArgs& ra;
-  const int lane, D;
+  const int lane;
+  int D, S, nJ;
+  bool hasH, hasEx, hasFreq, anySpecial;
+  const int* col;
+  const C2* val;
+  const double2* freq;
+  const double* jw;
   C2* buf0;
   C2* buf1;
   C2* cache;
+  WarpScratch* ws;
 
-  // register-resident operator rows
+  // Coefficients live in registers when E * SMAX is small (CREG), else they are
+  // re-read per right-hand side through L1 (shared by all trajectories of the system).
+  static constexpr bool CREG = E * SMAX <= 8;
   C2 diag[E];
-  C2 val[E * SMAX <= 8 ? SMAX : 1][E];
-  int col[E * SMAX <= 8 ? SMAX : 1][E];
+  C2 cval[CREG ? SMAX : 1][E];
+  int ccol[CREG ? SMAX : 1][E];
 
-  // state
+  // trajectory state
   C2 x[E];
   double t, t0, dtTry, dtDid;
-  Pcg64 pcg;
-  unsigned long long draws;
   unsigned long long ti;
-  unsigned long long nSteps, nAttempts, nFailed, nRhs, nOvershot, nBacks, nJumps;
+  // per-launch counter increments
+  unsigned nSteps, nAttempts, nFailed, nRhs, nOvershot, nBacks, nJumps;
   double maxOvershoot, maxTolOvershoot, maxNormDev;
   unsigned status;
 
-  __device__ Worker(const SysDev& s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c)
-      : sys(s), ra(a), lane(l), D(s.D), buf0(b0), buf1(b1), cache(c) {}
+  __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w)
+      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w) {
+    D = s->D;
+    S = s->S;
+    nJ = s->nJ;
+    hasH = s->hasH != 0;
+    hasEx = s->hasEx != 0;
+    hasFreq = s->hasFreq != 0;
+    col = s->col;
+    val = Tables<R>::val(*s);
+    freq = s->freq;
+    jw = s->jw;
+    anySpecial = false;
+    for (int m = 0; m < nJ; ++m) anySpecial |= !s->jHasW[m];
+  }
 
   __device__ __forceinline__ int row(int e) const { return lane + 32 * e; }
   __device__ __forceinline__ bool valid(int e) const { return row(e) < D; }
 
-  // Coefficients live in registers when E * SMAX is small (CREG), else they are
-  // re-read per right-hand side from global memory (L1-resident, shared by every
-  // trajectory of the system on the SM).
-  static constexpr bool CREG = E * SMAX <= 8;
-
-  __device__ void loadOperator() {
-    const C2* dg = Tables<R>::diag(sys);
-    const C2* vl = Tables<R>::val(sys);
+  __device__ __forceinline__ void loadOperator() {
+    const C2* dg = Tables<R>::diag(*sysp);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int r = row(e);
@@ -248,9 +291,9 @@ struct Worker {
       if constexpr (CREG) {
 #pragma unroll
         for (int s = 0; s < SMAX; ++s) {
-          const bool vs = v && s < sys.S;
-          col[s][e] = vs ? sys.col[s * D + r] : 0;
-          val[s][e] = vs ? vl[s * D + r] : mk<C2>(0, 0);
+          const bool vs = v && s < S;
+          ccol[s][e] = vs ? col[s * D + r] : 0;
+          cval[s][e] = vs ? val[s * D + r] : mk<C2>(0, 0);
         }
       }
     }
@@ -269,18 +312,18 @@ struct Worker {
       const int r = valid(e) ? row(e) : 0;
 #pragma unroll
       for (int s = 0; s < SMAX; ++s) {
-        if (s < sys.S) {
+        if (s < S) {
           C2 c;
           int cc;
           if constexpr (CREG) {
-            c = val[s][e];
-            cc = col[s][e];
+            c = cval[s][e];
+            cc = ccol[s][e];
           } else {
-            c = valid(e) ? __ldg(&Tables<R>::val(sys)[s * D + r]) : mk<C2>(0, 0);
-            cc = __ldg(&sys.col[s * D + r]);
+            c = valid(e) ? __ldg(&val[s * D + r]) : mk<C2>(0, 0);
+            cc = __ldg(&col[s * D + r]);
           }
-          if (sys.hasFreq && valid(e)) {
-            const double2 f = sys.freq[s * D + r];
+          if (hasFreq && valid(e)) {
+            const double2 f = __ldg(&freq[s * D + r]);
             if (f.x != 0. || f.y != 0.) {
               const double2 ph = cexpScaled(tau, f);
               c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
@@ -293,12 +336,14 @@ struct Worker {
     }
   }
 
-  // one adaptive ODE step towards at most deltaT (ode_engine::Base::step)
-  __device__ bool odeStep(double deltaT) {
+  // one adaptive ODE step towards at most deltaT (ode_engine::Base::step, ODE.h:234-262,
+  // with Boost.Odeint's controlled_runge_kutta<runge_kutta_cash_karp54>::try_step)
+  __device__ __forceinline__ bool odeStep(double deltaT) {
     const double timeBefore = t;
     const double nextDtTry = fabs(deltaT) < fabs(dtTry / 10.) ? dtTry : 0.;
     if (fabs(dtTry) > fabs(deltaT)) dtTry = deltaT;
     C2 k0[E], k1[E], k2[E], k3[E], k4[E], k5[E], y[E];
+    // dxdt at the start is the same for every attempt (Odeint recomputes it per try)
     rhs(x, k0, t - t0, buf0);
     for (int attempt = 0;; ++attempt) {
       if (attempt >= ra.maxAttempts) {
@@ -307,9 +352,11 @@ struct Worker {
       }
       ++nAttempts;
       const double dt = dtTry;
-      const R s10 = R(dt * CK::a10);
+      {
+        const R s0 = R(dt * CK::a10);
 #pragma unroll
-      for (int e = 0; e < E; ++e) y[e] = axpy(s10, k0[e], x[e]);
+        for (int e = 0; e < E; ++e) y[e] = axpy(s0, k0[e], x[e]);
+      }
       rhs(y, k1, t + CK::c1 * dt - t0, buf1);
       {
         const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
@@ -338,9 +385,10 @@ struct Worker {
           y[e] = axpy(s4, k4[e], axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])))));
       }
       rhs(y, k5, t + CK::c5 * dt - t0, buf1);
-      // 5th-order solution, embedded error and the Odeint error norm
+      // 5th-order solution, embedded error and the Odeint error norm (max over rows)
       const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
-      const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4), e5 = R(dt * CK::e5);
+      const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
+              e5 = R(dt * CK::e5);
       const double adt = fabs(dt);
       double errLocal = 0.;
 #pragma unroll
@@ -359,7 +407,7 @@ struct Worker {
         return false;
       }
       if (err > 1.0) {
-        dtTry = dt * fmax(0.9 * pow(err, -1. / 3.), 0.2);
+        dtTry = decreasedStep(dt, err);
         ++nFailed;
         if (!(dtTry > 0.) || t + dtTry == t) {
           status |= 4u;  // CQG_TRAJ_DT_UNDERFLOW
@@ -369,11 +417,7 @@ struct Worker {
         continue;
       }
       t += dt;
-      if (err < 0.5) {
-        err = fmax(3.2e-4, err);  // 5^-5
-        dtTry = dt * 0.9 * pow(err, -1. / 5.);
-      } else
-        dtTry = dt;
+      dtTry = err < 0.5 ? increasedStep(dt, err) : dt;
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = y[e];
       break;
@@ -383,29 +427,75 @@ struct Worker {
     return true;
   }
 
-  __device__ bool coherentTimeDevelopment(double Dt, bool li) {
-    if (sys.hasH) {
+  // (J_m psi) rows into out; psi staged in buf (caller synchronised)
+  __device__ __forceinline__ void applyJump(int m, const C2* buf, C2 (&out)[E]) const {
+    const int SJ = sysp->SJ;
+    const C2* jv = Tables<R>::jval(*sysp) + size_t(m) * SJ * D;
+    const int* jc = sysp->jcol + size_t(m) * SJ * D;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      C2 acc = mk<C2>(0, 0);
+      if (valid(e))
+        for (int s = 0; s < SJ; ++s) acc = cfma(jv[s * D + row(e)], buf[jc[s * D + row(e)]], acc);
+      out[e] = acc;
+    }
+  }
+
+  // Coherent part of MCWF_Trajectory::step (coherentTimeDevelopment, MCWF_Trajectory.h:250-276)
+  // fused with the rates of the renormalised state (:357-358): one warp reduction yields
+  // ||psi||^2 and every sum_n w_n |psi_n|^2 (or ||J psi||^2), and rate = raw / ||psi||^2.
+  __device__ __forceinline__ bool coherentAndRates(double Dt, bool li, double (&rates)[MAX_JUMPS]) {
+    if (hasH) {
       if (!odeStep(Dt)) return false;
     } else {
       const double stepToDo = li ? fmin(dtTry, Dt) : Dt;
       t += stepToDo;
       dtDid = stepToDo;
     }
-    if (sys.hasEx) {
+    if (hasEx) {
       const double tau = t - t0;
 #pragma unroll
       for (int e = 0; e < E; ++e)
         if (valid(e)) {
-          const double2 u = cexpScaled(tau, sys.lambda[row(e)]);
+          const double2 u = cexpScaled(tau, __ldg(&sysp->lambda[row(e)]));
           x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
         }
       t0 = t;
     }
-    double n2 = 0.;
+    double red[MAX_JUMPS + 1];
+    red[0] = 0.;
 #pragma unroll
-    for (int e = 0; e < E; ++e) n2 += abs2(x[e]);
-    n2 = warpSum(n2);
-    const double n = sqrt(n2);
+    for (int e = 0; e < E; ++e) red[0] += abs2(x[e]);
+    int nRed = 1;
+    if (li) {
+      if (anySpecial) {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (valid(e)) buf0[row(e)] = x[e];
+        __syncwarp();
+      }
+#pragma unroll
+      for (int m = 0; m < MAX_JUMPS; ++m) {
+        red[m + 1] = 0.;
+        if (m < nJ) {
+          if (!anySpecial || sysp->jHasW[m]) {
+            const double* w = jw + size_t(m) * D;
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+              if (valid(e)) red[m + 1] += __ldg(&w[row(e)]) * abs2(x[e]);
+          } else {
+            C2 jx[E];
+            applyJump(m, buf0, jx);
+#pragma unroll
+            for (int e = 0; e < E; ++e) red[m + 1] += abs2(jx[e]);
+          }
+        }
+      }
+      if (anySpecial) __syncwarp();
+      nRed = 1 + nJ;
+    }
+    warpSumN(red, nRed);
+    const double n = sqrt(red[0]);
     if (!(n > 0.) || !isfinite(n)) {
       status |= 1u;  // CQG_TRAJ_NONFINITE_NORM
       return false;
@@ -414,61 +504,28 @@ struct Worker {
 #pragma unroll
     for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(x[e].x) * inv, double(x[e].y) * inv);
     maxNormDev = fmax(maxNormDev, fabs(1. - n));
+    if (li) {
+      bool ok = true;
+      const double inv2 = 1. / red[0];
+#pragma unroll
+      for (int m = 0; m < MAX_JUMPS; ++m) {
+        rates[m] = m < nJ ? red[m + 1] * inv2 : 0.;
+        ok &= isfinite(rates[m]);
+      }
+      if (!ok) {
+        status |= 2u;  // CQG_TRAJ_NONFINITE_RATE
+        return false;
+      }
+    }
     return true;
   }
 
-  // (J_m psi) rows into out; psi staged in buf (caller synchronised)
-  __device__ __forceinline__ void applyJump(int m, const C2* buf, C2 (&out)[E]) const {
-    const C2* jv = Tables<R>::jval(sys) + size_t(m) * sys.SJ * D;
-    const int* jc = sys.jcol + size_t(m) * sys.SJ * D;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      C2 acc = mk<C2>(0, 0);
-      if (valid(e))
-        for (int s = 0; s < sys.SJ; ++s) acc = cfma(jv[s * D + row(e)], buf[jc[s * D + row(e)]], acc);
-      out[e] = acc;
-    }
-  }
-
-  __device__ bool computeRates(double (&rates)[MAX_JUMPS]) {
-    double part[MAX_JUMPS];
-    bool anySpecial = false;
-    for (int m = 0; m < sys.nJ; ++m) anySpecial |= !sys.jHasW[m];
-    if (anySpecial) {
-#pragma unroll
-      for (int e = 0; e < E; ++e)
-        if (valid(e)) buf0[row(e)] = x[e];
-      __syncwarp();
-    }
-    for (int m = 0; m < sys.nJ; ++m) {
-      double acc = 0.;
-      if (sys.jHasW[m]) {
-        const double* w = sys.jw + size_t(m) * D;
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-          if (valid(e)) acc += w[row(e)] * abs2(x[e]);
-      } else {
-        C2 jx[E];
-        applyJump(m, buf0, jx);
-#pragma unroll
-        for (int e = 0; e < E; ++e) acc += abs2(jx[e]);
-      }
-      part[m] = acc;
-    }
-    if (anySpecial) __syncwarp();
-    bool ok = true;
-    for (int m = 0; m < sys.nJ; ++m) {
-      rates[m] = warpSum(part[m]);
-      ok &= isfinite(rates[m]);
-    }
-    if (!ok) status |= 2u;  // CQG_TRAJ_NONFINITE_RATE
-    return ok;
-  }
-
-  // MCWF_Trajectory::manageTimeStep; true = step back
-  __device__ bool manageTimeStep(const double (&rates)[MAX_JUMPS], double tCache, double dtDidCache) {
+  // MCWF_Trajectory::manageTimeStep (MCWF_Trajectory.h:294-317); true = step back
+  __device__ __forceinline__ bool manageTimeStep(const double (&rates)[MAX_JUMPS], double tCache, double dtDidCache) {
     double totalRate = 0.;
-    for (int m = 0; m < sys.nJ; ++m) totalRate += rates[m];
+#pragma unroll
+    for (int m = 0; m < MAX_JUMPS; ++m)
+      if (m < nJ) totalRate += rates[m];
     const double liouvilleanSuggestedDtTry = ra.dpLimit / totalRate;
     if (totalRate * dtDid > ra.overTol * ra.dpLimit) {
       maxTolOvershoot = fmax(maxTolOvershoot, totalRate * dtDid);
@@ -481,29 +538,45 @@ struct Worker {
       ++nOvershot;
       maxOvershoot = fmax(maxOvershoot, totalRate * dtTry);
     }
-    dtTry = sys.hasH ? fmin(dtTry, liouvilleanSuggestedDtTry) : liouvilleanSuggestedDtTry;
+    dtTry = hasH ? fmin(dtTry, liouvilleanSuggestedDtTry) : liouvilleanSuggestedDtTry;
     return false;
   }
 
-  __device__ double uniform() {
+  __device__ __forceinline__ double uniform() {
     double u = 0.;
     if (lane == 0) {
-      if (ra.rng == 0)
-        u = canonicalFromU64(pcg.next());
-      else
-        u = philoxUniform(ra.seed, ti, draws);
+      if (ra.rng == 0) {
+        Pcg64 g;
+        g.state.hi = ws->pcg[0];
+        g.state.lo = ws->pcg[1];
+        g.inc.hi = ws->pcg[2];
+        g.inc.lo = ws->pcg[3];
+        u = canonicalFromU64(g.next());
+        ws->pcg[0] = g.state.hi;
+        ws->pcg[1] = g.state.lo;
+      } else {
+        u = philoxUniform(ra.seed, ti, ws->pcg[0]++);
+      }
     }
-    ++draws;
     return __shfl_sync(FULL, u, 0);
   }
 
-  __device__ bool performJump(const double (&rates)[MAX_JUMPS], const TrajDev& td) {
+  // MCWF_Trajectory::performJump (MCWF_Trajectory.h:320-344)
+  __device__ __forceinline__ bool performJump(const double (&rates)[MAX_JUMPS], const TrajDev& td) {
     double random = uniform() / dtDid;
-    int lindbladNo = 0;
-    for (; random > 0 && lindbladNo != sys.nJ; random -= rates[lindbladNo++])
-      ;
+    // for (; random > 0 && lindbladNo != nJ; random -= rates[lindbladNo++]) with static indices
+    int lindbladNo = -1;
+    double rate = 0.;
+#pragma unroll
+    for (int m = 0; m < MAX_JUMPS; ++m)
+      if (m < nJ && lindbladNo < 0 && random > 0) {
+        random -= rates[m];
+        if (!(random > 0)) {
+          lindbladNo = m;
+          rate = rates[m];
+        }
+      }
     if (random < 0) {
-      --lindbladNo;
 #pragma unroll
       for (int e = 0; e < E; ++e)
         if (valid(e)) buf0[row(e)] = x[e];
@@ -511,7 +584,7 @@ struct Worker {
       C2 jx[E];
       applyJump(lindbladNo, buf0, jx);
       __syncwarp();
-      const double normFactor = sqrt(rates[lindbladNo]);
+      const double normFactor = sqrt(rate);
       if (!isfinite(normFactor) || !(normFactor > 0.)) {
         status |= 1u;
         return false;
@@ -520,7 +593,8 @@ struct Worker {
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(jx[e].x) * inv, double(jx[e].y) * inv);
       if (lane == 0 && td.jumpCap > 0) {
-        const unsigned long long slot = nJumps % (unsigned long long)td.jumpCap;
+        const unsigned long long total = td.jumpN[ti] + nJumps;
+        const unsigned long long slot = total % (unsigned long long)td.jumpCap;
         td.jumpT[ti * td.jumpCap + slot] = t;
         td.jumpL[ti * td.jumpCap + slot] = lindbladNo;
       }
@@ -529,19 +603,18 @@ struct Worker {
     return true;
   }
 
-  // MCWF_Trajectory::step
-  __device__ bool step(double Dt, const TrajDev& td) {
-    const bool li = ra.noise && sys.nJ > 0;
+  // MCWF_Trajectory::step (MCWF_Trajectory.h:347-374)
+  __device__ __forceinline__ bool step(double Dt, const TrajDev& td) {
+    const bool li = ra.noise && nJ > 0;
     const double tCache = t, dtDidCache = dtDid;
     if (li) {
 #pragma unroll
       for (int e = 0; e < E; ++e)
         if (valid(e)) cache[row(e)] = x[e];
     }
-    if (!coherentTimeDevelopment(Dt, li)) return false;
+    double rates[MAX_JUMPS];
+    if (!coherentAndRates(Dt, li, rates)) return false;
     if (li) {
-      double rates[MAX_JUMPS];
-      if (!computeRates(rates)) return false;
       int backs = 0;
       while (manageTimeStep(rates, tCache, dtDidCache)) {
         if (++backs > 10000) {
@@ -551,8 +624,7 @@ struct Worker {
 #pragma unroll
         for (int e = 0; e < E; ++e)
           if (valid(e)) x[e] = cache[row(e)];
-        if (!coherentTimeDevelopment(Dt, li)) return false;
-        if (!computeRates(rates)) return false;
+        if (!coherentAndRates(Dt, li, rates)) return false;
       }
       if (!performJump(rates, td)) return false;
     }
@@ -560,21 +632,22 @@ struct Worker {
     return true;
   }
 
-  // per-trajectory linear averages <psi|O_k|psi>
-  __device__ void averages(double* out) {
+  // per-trajectory linear averages <psi|O_k|psi> (output times only)
+  __device__ __forceinline__ void averages(double* out) {
 #pragma unroll
     for (int e = 0; e < E; ++e)
       if (valid(e)) buf0[row(e)] = x[e];
     __syncwarp();
-    for (int k = 0; k < sys.nObs; ++k) {
-      const double2* ov = sys.oval + size_t(k) * sys.SO * D;
-      const int* oc = sys.ocol + size_t(k) * sys.SO * D;
+    const int nObs = sysp->nObs, SO = sysp->SO;
+    for (int k = 0; k < nObs; ++k) {
+      const double2* ov = sysp->oval + size_t(k) * SO * D;
+      const int* oc = sysp->ocol + size_t(k) * SO * D;
       double re = 0., im = 0.;
 #pragma unroll
       for (int e = 0; e < E; ++e)
         if (valid(e)) {
           double2 acc = make_double2(0., 0.);
-          for (int s = 0; s < sys.SO; ++s) {
+          for (int s = 0; s < SO; ++s) {
             const C2 v = buf0[oc[s * D + row(e)]];
             acc = cfma(ov[s * D + row(e)], make_double2(double(v.x), double(v.y)), acc);
           }
@@ -585,14 +658,15 @@ struct Worker {
       re = warpSum(re);
       im = warpSum(im);
       if (lane == 0 && out) {
-        if (sys.oRe[k] >= 0) out[sys.oRe[k]] = re;
-        if (sys.oIm[k] >= 0) out[sys.oIm[k]] = im;
+        const int cr = sysp->oRe[k], ci = sysp->oIm[k];
+        if (cr >= 0) out[cr] = re;
+        if (ci >= 0) out[ci] = im;
       }
     }
     __syncwarp();
   }
 
-  __device__ void run(const TrajDev& td, int trajIndex) {
+  __device__ __forceinline__ void run(const TrajDev& td, int trajIndex) {
     ti = (unsigned long long)trajIndex;
     C2* psi = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
     loadOperator();
@@ -602,20 +676,9 @@ struct Worker {
     t0 = td.t0[ti];
     dtTry = td.dtTry[ti];
     dtDid = td.dtDid[ti];
-    const unsigned long long* rs = td.rng + 4 * ti;
-    pcg.state.hi = rs[0];
-    pcg.state.lo = rs[1];
-    pcg.inc.hi = rs[2];
-    pcg.inc.lo = rs[3];
-    draws = rs[0];  // philox keeps its draw counter in word 0
-    const unsigned long long* c = td.cnt + 8 * ti;
-    nSteps = c[0];
-    nAttempts = c[1];
-    nFailed = c[2];
-    nRhs = c[3];
-    nOvershot = c[4];
-    nBacks = c[5];
-    nJumps = c[6];
+    if (lane < 4) ws->pcg[lane] = td.rng[4 * ti + lane];
+    __syncwarp();
+    nSteps = nAttempts = nFailed = nRhs = nOvershot = nBacks = nJumps = 0;
     maxOvershoot = td.maxima[3 * ti];
     maxTolOvershoot = td.maxima[3 * ti + 1];
     maxNormDev = td.maxima[3 * ti + 2];
@@ -652,35 +715,29 @@ struct Worker {
 #pragma unroll
     for (int e = 0; e < E; ++e)
       if (valid(e)) psi[row(e)] = x[e];
+    __syncwarp();
+    if (lane < 4) td.rng[4 * ti + lane] = ws->pcg[lane];
     if (lane == 0) {
       td.t[ti] = t;
       td.t0[ti] = t0;
       td.dtTry[ti] = dtTry;
       td.dtDid[ti] = dtDid;
-      unsigned long long* rw = td.rng + 4 * ti;
-      if (ra.rng == 0) {
-        rw[0] = pcg.state.hi;
-        rw[1] = pcg.state.lo;
-        rw[2] = pcg.inc.hi;
-        rw[3] = pcg.inc.lo;
-      } else {
-        rw[0] = draws;
-      }
       unsigned long long* cw = td.cnt + 8 * ti;
-      cw[0] = nSteps;
-      cw[1] = nAttempts;
-      cw[2] = nFailed;
-      cw[3] = nRhs;
-      cw[4] = nOvershot;
-      cw[5] = nBacks;
-      cw[6] = nJumps;
+      cw[0] += nSteps;
+      cw[1] += nAttempts;
+      cw[2] += nFailed;
+      cw[3] += nRhs;
+      cw[4] += nOvershot;
+      cw[5] += nBacks;
+      cw[6] += nJumps;
       cw[7] = status;
       td.maxima[3 * ti] = maxOvershoot;
       td.maxima[3 * ti + 1] = maxTolOvershoot;
       td.maxima[3 * ti + 2] = maxNormDev;
       td.status[ti] = status;
-      if (td.jumpN) td.jumpN[ti] = nJumps;
+      td.jumpN[ti] += nJumps;
     }
+    __syncwarp();
   }
 };
 
@@ -691,16 +748,16 @@ __global__ void __launch_bounds__(128) mcwfWarpKernel(TrajDev td, RunArgs ra) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int DMAX = 32 * E;
   C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * 3 * DMAX;
+  WarpScratch* ws =
+      reinterpret_cast<WarpScratch*>(smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) + warp;
   while (true) {
     int task = 0;
     if (lane == 0) task = atomicAdd(ra.queue, 1);
     task = __shfl_sync(FULL, task, 0);
     if (task >= td.nTraj) return;
     const int ti = ra.order ? ra.order[task] : task;
-    const SysDev& sys = td.systems[td.sysIdx[ti]];
-    Worker<R, E, SMAX> w(sys, ra, lane, base, base + DMAX, base + 2 * DMAX);
+    Worker<R, E, SMAX> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws);
     w.run(td, ti);
-    __syncwarp();
   }
 }
 
