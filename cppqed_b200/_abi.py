@@ -138,6 +138,7 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
     "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
     "cqg_ensemble_destroy": (C.c_int, [_P]),
+    "cqg_system_averages_noalloc": (C.c_int, [_P, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "cqg_model_create": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(_P)]),
     "cqg_model_desc": (C.c_int, [_P, C.POINTER(C.POINTER(cqg_system_desc))]),
     "cqg_model_dimension": (C.c_int, [_P, C.POINTER(C.c_int64)]),

@@ -558,6 +558,14 @@ double probe(int device) {
 
 }  // namespace
 
+namespace cqg {
+namespace dev {
+// accessors for the allocation-free averages entry point (noalloc.cu)
+const SysDev* systemDescriptor(const cqg_system* sys) { return &sys->sd; }
+int systemDevice(const cqg_system* sys) { return sys->device; }
+}  // namespace dev
+}  // namespace cqg
+
 extern "C" {
 
 int cqg_device_count(int* count) {

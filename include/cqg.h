@@ -227,6 +227,24 @@ int cqg_probe_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 
 int cqg_ensemble_destroy(cqg_ensemble* ens);
 
+/* ---- allocation-free averages ---------------------------------------------
+ * No counterpart in the reference.  Sums over n_states caller-owned device states
+ * (psi: n_states x D complex128, C-order, state after state) of the system's linear
+ * averages: sums[c] = sum_i Re/Im <psi_i|O|psi_i>, the columns of cqg_ensemble_run
+ * without the dtDid column.  For callers that cannot allocate device memory — their
+ * memory belongs to another allocator (a framework pool, a serving runtime that
+ * reserved the GPU up front) or they run where cudaMalloc is not allowed or would
+ * synchronise the device.  Allocates nothing: the per-state intermediate sums live in
+ * one fixed device array of 2^18 doubles held by every GPU that loads the library, so
+ * n_states * n_avr must not exceed 262144 (larger requests fail with CQG_E_INVALID).
+ * psi and sums are device pointers; work is queued on `stream` (a cudaStream_t, NULL
+ * for the default stream) and the call returns without waiting.  The first call on a
+ * device looks up the array's device address, so make that first call before any
+ * stream capture.  All calls share the array: calls whose work overlaps on the GPU
+ * race and give wrong sums.  The current device must be the system's device. */
+int cqg_system_averages_noalloc(const cqg_system* sys, const cqg_complex* psi, int64_t n_states, double* sums,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif
