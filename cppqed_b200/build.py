@@ -18,10 +18,10 @@ LIB = os.path.join(LIBDIR, "libcqg.so")
 
 HOST_SOURCES = ["host/tridiagonal.cpp", "host/elements.cpp", "host/model.cpp", "host/pars.cpp",
                 "host/scripts.cpp", "host/errors.cpp", "host/api_model.cpp", "host/lowering.cpp"]
-CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu"]
+CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu", "cuda/kernels_block.cu"]
 # the kernel instantiations: one object per (precision, rows per lane)
 KERNEL_INSTANCES = [(r, e) for r in ("double", "float") for e in (1, 2, 3, 4)]
-HEADERS = ["cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
+HEADERS = ["cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/mcwf_block.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
            "host/elements.hpp", "host/tridiagonal.hpp", "host/pars.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -48,7 +48,7 @@ def _run(cmd, verbose):
     return r.stdout + r.stderr
 
 
-def build(verbose=False, ptxas_info=False):
+def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     inc = ["-I" + os.path.join(ROOT, "include")]
@@ -75,8 +75,8 @@ def build(verbose=False, ptxas_info=False):
     for s, o, defs in jobs:
         objs.append(o)
         if _stale(o, [s] + headers) or ptxas_info:
-            cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs, "-c", s,
-                   "-o", o]
+            cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs,
+                   *extra_flags, "-c", s, "-o", o]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             if verbose:
@@ -88,8 +88,9 @@ def build(verbose=False, ptxas_info=False):
             sys.stderr.write(out)
             raise RuntimeError("build step failed: " + " ".join(cmd[:3]) + " ...")
         info += out
-    if _stale(LIB, objs):
-        _run([_nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"], verbose)
+    out = lib or LIB
+    if _stale(out, objs):
+        _run([_nvcc(), *ARCH, "-shared", "-o", out, *objs, "-lcudart"], verbose)
     return info
 
 

@@ -14,6 +14,7 @@
 #include "../host/errors.hpp"
 #include "../host/lowering.hpp"
 #include "cqg.h"
+#include "mcwf_block.cuh"
 #include "mcwf_kernel.cuh"
 
 using cqg::fail;
@@ -87,8 +88,11 @@ struct cqg_ensemble {
   size_t avrCap = 0;
   double* dSums = nullptr;
   size_t sumsCap = 0;
+  void* dBlockScratch = nullptr;  // per-CTA stage vectors of the block kernel
+  size_t blockScratchBytes = 0;
   int jumpCap = 64;
   ~cqg_ensemble() {
+    if (dBlockScratch) cudaFree(dBlockScratch);
     if (dAvr) cudaFree(dAvr);
     if (dSums) cudaFree(dSums);
     if (dmem) cudaFree(dmem);
@@ -254,6 +258,20 @@ KernelFn pick_float_e4(int smax);
 
 namespace {
 
+}  // namespace
+
+namespace cqg {
+namespace dev {
+using BlockKernelFn = void (*)(TrajDev, RunArgs, BlockScratch, int);
+BlockKernelFn pick_block(bool fp64);
+}  // namespace dev
+}  // namespace cqg
+
+namespace {
+
+// the warp kernel holds up to 4 rows per lane
+constexpr int kWarpKernelMaxD = 128;
+
 KernelFn pickKernel(bool fp64, int E, int SMAX) {
   if (fp64)
     return E == 1 ? dev::pick_double_e1(SMAX)
@@ -311,7 +329,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     if (int(systems[s]->L.jumps.size()) > dev::MAX_JUMPS)
       return fail(CQG_E_UNSUPPORTED, "ensemble: more than 8 jump operators");
   }
-  if (e->Dmax > 128) return fail(CQG_E_UNSUPPORTED, "ensemble: total dimension above 128 is not supported by the warp kernel");
+  if (int64_t(e->Dmax) * 2 * (pars->precision == CQG_FP64 ? 16 : 8) > 200 * 1024)
+    return fail(CQG_E_UNSUPPORTED, "ensemble: the stage vectors of a trajectory exceed shared memory");
   if (e->Smax > 8) return fail(CQG_E_UNSUPPORTED, "ensemble: more than 8 off-diagonal entries per row");
   e->device = systems[0]->device;
   ck(cudaSetDevice(e->device), "cudaSetDevice");
@@ -466,24 +485,54 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   ra.maxStepsPerInterval = 2000000000LL;
   ra.timeLimitNs = 120ull * 1000000000ull;
 
-  const int E = (e->Dmax + 31) / 32;  // rows per lane, 1..4
-  const int SM = e->Smax <= 2 ? 2 : e->Smax <= 4 ? 4 : 8;
-  KernelFn fn = pickKernel(e->pars.precision == CQG_FP64, E, SM);
-  const int threads = 128;
-  const size_t smem =
-      size_t(threads / 32) * 3 * 32 * E * e->elemBytes + size_t(threads / 32) * sizeof(dev::WarpScratch);
-  ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-     "cudaFuncSetAttribute");
-  int perSM = 0, nSM = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem), "occupancy");
+  int nSM = 0;
   ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e->device), "attribute");
-  const int64_t warpsNeeded = e->nTraj;
-  int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (warpsNeeded + 3) / 4));
-  grid = std::max(grid, 1);
-  ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
-  {
+  if (e->Dmax <= kWarpKernelMaxD) {
+    const int E = (e->Dmax + 31) / 32;  // rows per lane, 1..4
+    KernelFn fn = pickKernel(e->pars.precision == CQG_FP64, E, e->Smax);
+    const int threads = 128;
+    const size_t smem =
+        size_t(threads / 32) * 3 * 32 * E * e->elemBytes + size_t(threads / 32) * sizeof(dev::WarpScratch);
+    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+       "cudaFuncSetAttribute");
+    int perSM = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem),
+       "occupancy");
+    const int64_t warpsNeeded = e->nTraj;
+    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (warpsNeeded + 3) / 4));
+    grid = std::max(grid, 1);
+    ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
     dev::TrajDev tdArg = e->td;
     void* args[] = {&tdArg, &ra};
+    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(threads), args, smem, e->stream),
+       "kernel launch");
+  } else {
+    // one CTA per trajectory: stage vectors in shared memory, stage derivatives in a
+    // per-CTA scratch slab
+    dev::BlockKernelFn fn = dev::pick_block(e->pars.precision == CQG_FP64);
+    const int threads = 256;
+    int smemD = e->Dmax;
+    const size_t smem = 2 * size_t(smemD) * e->elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+       "cudaFuncSetAttribute");
+    int perSM = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem),
+       "occupancy");
+    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, e->nTraj));
+    grid = std::max(grid, 1);
+    dev::BlockScratch bsc;
+    bsc.stride = (e->Dmax + 31) / 32 * 32;
+    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * e->elemBytes;
+    if (need > e->blockScratchBytes) {
+      if (e->dBlockScratch) cudaFree(e->dBlockScratch);
+      e->dBlockScratch = nullptr;
+      ck(cudaMalloc(&e->dBlockScratch, need), "cudaMalloc(block scratch)");
+      e->blockScratchBytes = need;
+    }
+    bsc.base = e->dBlockScratch;
+    ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
+    dev::TrajDev tdArg = e->td;
+    void* args[] = {&tdArg, &ra, &bsc, &smemD};
     ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(threads), args, smem, e->stream),
        "kernel launch");
   }

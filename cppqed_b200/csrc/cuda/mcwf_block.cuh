@@ -1,0 +1,503 @@
+// MCWF trajectory kernel for large Hilbert spaces (D > 128), one CTA per trajectory.
+//
+// The warp kernel keeps a trajectory's state and stage derivatives in registers, which
+// limits it to D <= 128.  Here a CTA owns one trajectory at a time (persistent CTAs pull
+// trajectories from the same work queue) and each thread walks rows r = tid + blockDim*j.
+// The state stays in the trajectory's slot in device memory, the six Cash-Karp stage
+// derivatives, the candidate solution and the step-start cache live in a per-CTA scratch
+// slab (L2-resident for the CTAs in flight), and only the stage vector that the banded
+// H/i gather reads is staged in shared memory (double-buffered, one __syncthreads per
+// right-hand side).  Every row is touched by the same thread in every pass, so the
+// scratch vectors need no synchronisation.  The algorithm, step by step, is the one of
+// the warp kernel (mcwf_kernel.cuh) and of the reference's MCWF_Trajectory::step.
+#pragma once
+
+#include "mcwf_kernel.cuh"
+
+namespace cqg {
+namespace dev {
+
+constexpr int kBlockVectors = 8;  // k0..k5, candidate solution, step-start cache
+
+// Cash-Karp stage tableau for the (not unrolled) stage loop
+__constant__ double kBlockA[5][5] = {{1. / 5, 0, 0, 0, 0},
+                                     {3. / 40, 9. / 40, 0, 0, 0},
+                                     {3. / 10, -9. / 10, 6. / 5, 0, 0},
+                                     {-11. / 54, 5. / 2, -70. / 27, 35. / 27, 0},
+                                     {1631. / 55296, 175. / 512, 575. / 13824, 44275. / 110592, 253. / 4096}};
+__constant__ double kBlockC[5] = {1. / 5, 3. / 10, 3. / 5, 1., 7. / 8};
+
+struct BlockScratch {
+  void* base;           // [gridDim.x][kBlockVectors][stride] Real2
+  long long stride;     // elements per vector (>= max D)
+};
+
+// block-wide sums of n <= N uniform values; red holds 32 * N doubles of shared memory
+template <int N>
+__device__ __forceinline__ void blockSumN(double (&v)[N], int n, double* red) {
+  warpSumN(v, n);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    for (int m = 0; m < n; ++m) red[warp * N + m] = v[m];
+  __syncthreads();
+  for (int m = 0; m < n; ++m) {
+    double s = 0.;
+    for (int w = 0; w < nw; ++w) s += red[w * N + m];
+    v[m] = s;
+  }
+}
+
+__device__ __forceinline__ double blockMax(double v, double* red) {
+  v = warpMax(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double m = 0.;
+  for (int w = 0; w < nw; ++w) m = fmax(m, red[w]);
+  return m;
+}
+
+template <typename R>
+struct BlockWorker {
+  using C2 = typename CT<R>::T;
+  static constexpr int NR = MAX_JUMPS + 1;
+
+  const SysDev* sysp;
+  const RunArgs& ra;
+  int D, S, nJ;
+  bool hasH, hasEx, hasFreq, anySpecial;
+  const int* col;
+  const C2* val;
+  const C2* diag;
+  const double2* freq;
+  C2* x;       // the trajectory's state (device memory)
+  C2* vec;     // this CTA's scratch vectors
+  long long stride;
+  C2* ys0;     // shared stage buffers
+  C2* ys1;
+  double* red; // shared reduction scratch [32][NR]
+  unsigned long long* bcast;  // shared broadcast words
+
+  double t, t0, dtTry, dtDid;
+  unsigned long long ti;
+  unsigned nSteps, nAttempts, nFailed, nRhs, nOvershot, nBacks, nJumps;
+  double maxOvershoot, maxTolOvershoot, maxNormDev;
+  unsigned status;
+
+  __device__ __forceinline__ C2* K(int j) const { return vec + j * stride; }
+  __device__ __forceinline__ C2* xnew() const { return vec + 6 * stride; }
+  __device__ __forceinline__ C2* cache() const { return vec + 7 * stride; }
+
+  // out = (H/i) y, y in shared memory
+  __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
+    ++nRhs;
+    for (int r = threadIdx.x; r < D; r += blockDim.x) {
+      C2 acc = cmul(diag[r], ys[r]);
+      for (int s = 0; s < S; ++s) {
+        C2 c = __ldg(&val[s * D + r]);
+        if (hasFreq) {
+          const double2 f = __ldg(&freq[s * D + r]);
+          if (f.x != 0. || f.y != 0.) {
+            const double2 ph = cexpScaled(tau, f);
+            c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+          }
+        }
+        acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
+      }
+      out[r] = acc;
+    }
+  }
+
+  __device__ __forceinline__ bool odeStep(double deltaT) {
+    const double timeBefore = t;
+    const double nextDtTry = fabs(deltaT) < fabs(dtTry / 10.) ? dtTry : 0.;
+    if (fabs(dtTry) > fabs(deltaT)) dtTry = deltaT;
+    __syncthreads();
+    for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
+    __syncthreads();
+    rhs(ys0, K(0), t - t0);
+    for (int attempt = 0;; ++attempt) {
+      if (attempt >= ra.maxAttempts) {
+        status |= 8u;
+        return false;
+      }
+      ++nAttempts;
+      const double dt = dtTry;
+      for (int st = 1; st <= 5; ++st) {
+        C2* ys = (st & 1) ? ys1 : ys0;
+        for (int r = threadIdx.x; r < D; r += blockDim.x) {
+          C2 y = x[r];
+          for (int j = 0; j < st; ++j) y = axpy(R(dt * kBlockA[st - 1][j]), K(j)[r], y);
+          ys[r] = y;
+        }
+        __syncthreads();
+        rhs(ys, K(st), t + kBlockC[st - 1] * dt - t0);
+      }
+      const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
+      const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
+              e5 = R(dt * CK::e5);
+      const double adt = fabs(dt);
+      double errLocal = 0.;
+      for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        const C2 xr = x[r], k0 = K(0)[r], k2 = K(2)[r], k3 = K(3)[r], k4 = K(4)[r], k5 = K(5)[r];
+        xnew()[r] = axpy(b5, k5, axpy(b3, k3, axpy(b2, k2, axpy(b0, k0, xr))));
+        C2 xe = mk<C2>(0, 0);
+        xe = axpy(e5, k5, axpy(e4, k4, axpy(e3, k3, axpy(e2, k2, axpy(e0, k0, xe)))));
+        const double den = ra.absSlot + ra.relSlot * (cabs(xr) + adt * cabs(k0));
+        errLocal = fmax(errLocal, cabs(xe) / den);
+      }
+      const double err = blockMax(errLocal, red);
+      if (!(err == err)) {
+        status |= 1u;
+        return false;
+      }
+      if (err > 1.0) {
+        dtTry = decreasedStep(dt, err);
+        ++nFailed;
+        if (!(dtTry > 0.) || t + dtTry == t) {
+          status |= 4u;
+          return false;
+        }
+        continue;
+      }
+      t += dt;
+      dtTry = err < 0.5 ? increasedStep(dt, err) : dt;
+      for (int r = threadIdx.x; r < D; r += blockDim.x) x[r] = xnew()[r];
+      break;
+    }
+    dtDid = t - timeBefore;
+    if (nextDtTry != 0.) dtTry = nextDtTry;
+    return true;
+  }
+
+  // J_m applied to the state staged in ys0 (caller synchronised), result into out
+  __device__ __forceinline__ void applyJump(int m, C2* out) const {
+    const int SJ = sysp->SJ;
+    const C2* jv = Tables<R>::jval(*sysp) + size_t(m) * SJ * D;
+    const int* jc = sysp->jcol + size_t(m) * SJ * D;
+    for (int r = threadIdx.x; r < D; r += blockDim.x) {
+      C2 acc = mk<C2>(0, 0);
+      for (int s = 0; s < SJ; ++s) acc = cfma(jv[s * D + r], ys0[jc[s * D + r]], acc);
+      out[r] = acc;
+    }
+  }
+
+  __device__ __forceinline__ bool coherentAndRates(double Dt, bool li, double (&rates)[MAX_JUMPS]) {
+    if (hasH) {
+      if (!odeStep(Dt)) return false;
+    } else {
+      const double stepToDo = li ? fmin(dtTry, Dt) : Dt;
+      t += stepToDo;
+      dtDid = stepToDo;
+    }
+    if (hasEx) {
+      const double tau = t - t0;
+      for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        const double2 u = cexpScaled(tau, __ldg(&sysp->lambda[r]));
+        const C2 v = x[r];
+        x[r] = mk<C2>(double(v.x) * u.x - double(v.y) * u.y, double(v.x) * u.y + double(v.y) * u.x);
+      }
+      t0 = t;
+    }
+    double v[NR];
+    for (int m = 0; m < NR; ++m) v[m] = 0.;
+    if (li && anySpecial) {
+      __syncthreads();
+      for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
+      __syncthreads();
+    }
+    for (int r = threadIdx.x; r < D; r += blockDim.x) v[0] += abs2(x[r]);
+    int nRed = 1;
+    if (li) {
+      for (int m = 0; m < nJ; ++m) {
+        double acc = 0.;
+        if (sysp->jHasW[m]) {
+          const double* w = sysp->jw + size_t(m) * D;
+          for (int r = threadIdx.x; r < D; r += blockDim.x) acc += __ldg(&w[r]) * abs2(x[r]);
+        } else {
+          const int SJ = sysp->SJ;
+          const C2* jv = Tables<R>::jval(*sysp) + size_t(m) * SJ * D;
+          const int* jc = sysp->jcol + size_t(m) * SJ * D;
+          for (int r = threadIdx.x; r < D; r += blockDim.x) {
+            C2 a = mk<C2>(0, 0);
+            for (int s = 0; s < SJ; ++s) a = cfma(jv[s * D + r], ys0[jc[s * D + r]], a);
+            acc += abs2(a);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < MAX_JUMPS; ++q)
+          if (q == m) v[q + 1] = acc;
+      }
+      nRed = 1 + nJ;
+    }
+    blockSumN(v, nRed, red);
+    const double n = sqrt(v[0]);
+    if (!(n > 0.) || !isfinite(n)) {
+      status |= 1u;
+      return false;
+    }
+    const double inv = 1. / n;
+    for (int r = threadIdx.x; r < D; r += blockDim.x) {
+      const C2 a = x[r];
+      x[r] = mk<C2>(double(a.x) * inv, double(a.y) * inv);
+    }
+    maxNormDev = fmax(maxNormDev, fabs(1. - n));
+    if (li) {
+      bool ok = true;
+      const double inv2 = 1. / v[0];
+#pragma unroll
+      for (int m = 0; m < MAX_JUMPS; ++m) {
+        rates[m] = m < nJ ? v[m + 1] * inv2 : 0.;
+        ok &= isfinite(rates[m]);
+      }
+      if (!ok) {
+        status |= 2u;
+        return false;
+      }
+    }
+    return true;
+  }
+
+  __device__ __forceinline__ bool manageTimeStep(const double (&rates)[MAX_JUMPS], double tCache, double dtDidCache) {
+    double totalRate = 0.;
+#pragma unroll
+    for (int m = 0; m < MAX_JUMPS; ++m)
+      if (m < nJ) totalRate += rates[m];
+    const double suggested = ra.dpLimit / totalRate;
+    if (totalRate * dtDid > ra.overTol * ra.dpLimit) {
+      maxTolOvershoot = fmax(maxTolOvershoot, totalRate * dtDid);
+      t = tCache;
+      dtDid = dtDidCache;
+      dtTry = suggested;
+      ++nBacks;
+      return true;
+    } else if (totalRate * dtTry > ra.dpLimit) {
+      ++nOvershot;
+      maxOvershoot = fmax(maxOvershoot, totalRate * dtTry);
+    }
+    dtTry = hasH ? fmin(dtTry, suggested) : suggested;
+    return false;
+  }
+
+  __device__ __forceinline__ double uniform() {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double u;
+      if (ra.rng == 0) {
+        Pcg64 g;
+        g.state.hi = bcast[0];
+        g.state.lo = bcast[1];
+        g.inc.hi = bcast[2];
+        g.inc.lo = bcast[3];
+        u = canonicalFromU64(g.next());
+        bcast[0] = g.state.hi;
+        bcast[1] = g.state.lo;
+      } else {
+        u = philoxUniform(ra.seed, ti, bcast[0]++);
+      }
+      reinterpret_cast<double*>(bcast)[4] = u;
+    }
+    __syncthreads();
+    return reinterpret_cast<double*>(bcast)[4];
+  }
+
+  __device__ __forceinline__ bool performJump(const double (&rates)[MAX_JUMPS], const TrajDev& td) {
+    double random = uniform() / dtDid;
+    int lindbladNo = -1;
+    double rate = 0.;
+#pragma unroll
+    for (int m = 0; m < MAX_JUMPS; ++m)
+      if (m < nJ && lindbladNo < 0 && random > 0) {
+        random -= rates[m];
+        if (!(random > 0)) {
+          lindbladNo = m;
+          rate = rates[m];
+        }
+      }
+    if (random < 0) {
+      for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
+      __syncthreads();
+      const double normFactor = sqrt(rate);
+      if (!isfinite(normFactor) || !(normFactor > 0.)) {
+        status |= 1u;
+        return false;
+      }
+      applyJump(lindbladNo, x);
+      const double inv = 1. / normFactor;
+      for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        const C2 a = x[r];
+        x[r] = mk<C2>(double(a.x) * inv, double(a.y) * inv);
+      }
+      if (threadIdx.x == 0 && td.jumpCap > 0) {
+        const unsigned long long total = td.jumpN[ti] + nJumps;
+        const unsigned long long slot = total % (unsigned long long)td.jumpCap;
+        td.jumpT[ti * td.jumpCap + slot] = t;
+        td.jumpL[ti * td.jumpCap + slot] = lindbladNo;
+      }
+      ++nJumps;
+    }
+    return true;
+  }
+
+  __device__ __forceinline__ bool step(double Dt, const TrajDev& td) {
+    const bool li = ra.noise && nJ > 0;
+    const double tCache = t, dtDidCache = dtDid;
+    if (li)
+      for (int r = threadIdx.x; r < D; r += blockDim.x) cache()[r] = x[r];
+    double rates[MAX_JUMPS];
+    if (!coherentAndRates(Dt, li, rates)) return false;
+    if (li) {
+      int backs = 0;
+      while (manageTimeStep(rates, tCache, dtDidCache)) {
+        if (++backs > 10000) {
+          status |= 8u;
+          return false;
+        }
+        for (int r = threadIdx.x; r < D; r += blockDim.x) x[r] = cache()[r];
+        if (!coherentAndRates(Dt, li, rates)) return false;
+      }
+      if (!performJump(rates, td)) return false;
+    }
+    ++nSteps;
+    return true;
+  }
+
+  __device__ __forceinline__ void averages(double* out) {
+    __syncthreads();
+    for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
+    __syncthreads();
+    const int nObs = sysp->nObs, SO = sysp->SO;
+    for (int k = 0; k < nObs; ++k) {
+      const double2* ov = sysp->oval + size_t(k) * SO * D;
+      const int* oc = sysp->ocol + size_t(k) * SO * D;
+      double v[2] = {0., 0.};
+      for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        double2 acc = make_double2(0., 0.);
+        for (int s = 0; s < SO; ++s) {
+          const C2 y = ys0[oc[s * D + r]];
+          acc = cfma(ov[s * D + r], make_double2(double(y.x), double(y.y)), acc);
+        }
+        const C2 xr = ys0[r];
+        v[0] += double(xr.x) * acc.x + double(xr.y) * acc.y;
+        v[1] += double(xr.x) * acc.y - double(xr.y) * acc.x;
+      }
+      blockSumN(v, 2, red);
+      if (threadIdx.x == 0 && out) {
+        const int cr = sysp->oRe[k], ci = sysp->oIm[k];
+        if (cr >= 0) out[cr] = v[0];
+        if (ci >= 0) out[ci] = v[1];
+      }
+    }
+  }
+
+  __device__ __forceinline__ void run(const TrajDev& td, int trajIndex) {
+    ti = (unsigned long long)trajIndex;
+    x = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
+    t = td.t[ti];
+    t0 = td.t0[ti];
+    dtTry = td.dtTry[ti];
+    dtDid = td.dtDid[ti];
+    if (threadIdx.x < 4) bcast[threadIdx.x] = td.rng[4 * ti + threadIdx.x];
+    nSteps = nAttempts = nFailed = nRhs = nOvershot = nBacks = nJumps = 0;
+    maxOvershoot = td.maxima[3 * ti];
+    maxTolOvershoot = td.maxima[3 * ti + 1];
+    maxNormDev = td.maxima[3 * ti + 2];
+    status = td.status[ti];
+    __syncthreads();
+
+    const int nOut = ra.mode == RUN_TO ? 1 : ra.nIntervals;
+    const unsigned long long tStart = globalTimerNs();
+    for (int k = 0; k < nOut && status == 0u; ++k) {
+      long long guard = 0;
+      if (ra.mode == RUN_STEPS) {
+        for (int s = 0; s < ra.nSteps && t < ra.T; ++s)
+          if (!step(ra.T - t, td)) break;
+      } else {
+        const double endTime = ra.mode == RUN_TO ? ra.tEnd : t + ra.Dt;
+        double dt;
+        while ((dt = endTime - t) != 0.) {
+          if (dt < 0. || ++guard > ra.maxStepsPerInterval ||
+              ((guard & 63) == 0 && globalTimerNs() - tStart > ra.timeLimitNs)) {
+            status |= 8u;
+            break;
+          }
+          if (!step(dt, td)) break;
+        }
+      }
+      if (ra.avrOut) {
+        double* slot = ra.avrOut + ((size_t)k * td.nTraj + ti) * ra.nAvrStride;
+        averages(slot);
+        if (threadIdx.x == 0) slot[ra.nAvrStride - 1] = dtDid;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) td.rng[4 * ti + threadIdx.x] = bcast[threadIdx.x];
+    if (threadIdx.x == 0) {
+      td.t[ti] = t;
+      td.t0[ti] = t0;
+      td.dtTry[ti] = dtTry;
+      td.dtDid[ti] = dtDid;
+      unsigned long long* cw = td.cnt + 8 * ti;
+      cw[0] += nSteps;
+      cw[1] += nAttempts;
+      cw[2] += nFailed;
+      cw[3] += nRhs;
+      cw[4] += nOvershot;
+      cw[5] += nBacks;
+      cw[6] += nJumps;
+      cw[7] = status;
+      td.maxima[3 * ti] = maxOvershoot;
+      td.maxima[3 * ti + 1] = maxTolOvershoot;
+      td.maxima[3 * ti + 2] = maxNormDev;
+      td.status[ti] = status;
+      td.jumpN[ti] += nJumps;
+    }
+    __syncthreads();
+  }
+};
+
+// Dynamic shared memory: two stage buffers of `smemD` elements, the reduction scratch,
+// then 8 broadcast words.
+template <typename R>
+__global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, BlockScratch bsc, int smemD) {
+  using C2 = typename CT<R>::T;
+  extern __shared__ __align__(16) unsigned char blockSmem[];
+  C2* ys0 = reinterpret_cast<C2*>(blockSmem);
+  C2* ys1 = ys0 + smemD;
+  double* red = reinterpret_cast<double*>(ys1 + smemD);
+  unsigned long long* bcast = reinterpret_cast<unsigned long long*>(red + 32 * (MAX_JUMPS + 1));
+  __shared__ int task;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) task = atomicAdd(ra.queue, 1);
+    __syncthreads();
+    if (task >= td.nTraj) return;
+    const int ti = ra.order ? ra.order[task] : task;
+    const SysDev* s = td.systems + td.sysIdx[ti];
+    BlockWorker<R> w{s, ra};
+    w.D = s->D;
+    w.S = s->S;
+    w.nJ = s->nJ;
+    w.hasH = s->hasH != 0;
+    w.hasEx = s->hasEx != 0;
+    w.hasFreq = s->hasFreq != 0;
+    w.anySpecial = false;
+    for (int m = 0; m < w.nJ; ++m) w.anySpecial |= !s->jHasW[m];
+    w.col = s->col;
+    w.val = Tables<R>::val(*s);
+    w.diag = Tables<R>::diag(*s);
+    w.freq = s->freq;
+    w.vec = reinterpret_cast<C2*>(bsc.base) + size_t(blockIdx.x) * kBlockVectors * bsc.stride;
+    w.stride = bsc.stride;
+    w.ys0 = ys0;
+    w.ys1 = ys1;
+    w.red = red;
+    w.bcast = bcast;
+    w.run(td, ti);
+  }
+}
+
+}  // namespace dev
+}  // namespace cqg

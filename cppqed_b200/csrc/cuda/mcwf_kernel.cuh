@@ -741,8 +741,12 @@ struct Worker {
   }
 };
 
+#ifndef CQG_MIN_BLOCKS
+#define CQG_MIN_BLOCKS 1
+#endif
+
 template <typename R, int E, int SMAX>
-__global__ void __launch_bounds__(128) mcwfWarpKernel(TrajDev td, RunArgs ra) {
+__global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td, RunArgs ra) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

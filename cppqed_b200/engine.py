@@ -12,7 +12,8 @@ import numpy as np
 from . import _abi as A
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libcqg.so")
+# the in-tree build; CQG_LIBRARY selects another build of the same library
+LIB_PATH = os.environ.get("CQG_LIBRARY") or os.path.join(_HERE, "_lib", "libcqg.so")
 _lib = None
 
 

@@ -152,3 +152,95 @@ def test_stalled_trajectory_reports_status(gpu):
     assert e.value.code == A.CQG_E_STALLED
     rc, bits = ens.status()
     assert bits & 8
+
+
+# ---- block-per-trajectory kernel (D > 128) ----------------------------------------
+
+def test_block_kernel_jump_free_trajectory_matches_oracle(gpu, oracle):
+    args = C2_ARGS[:]
+    args[args.index("--cutoff") + 1] = "100"  # D = 200
+    model = gpu.Model("QbitMode_C++QED", args + ["--no_noise"])
+    assert model.dim == 200
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), 2, pars)
+    for k in range(1, 4):
+        ens.run(0.2, 1)
+        ref = oracle.trajectory(model, pars, pars.prng_stream, 0.2, k)
+        for i in range(2):
+            psi = ens.state(i, model.dim)
+            assert np.linalg.norm(psi - ref["psi"]) <= 1e-10 * np.linalg.norm(ref["psi"])
+
+
+def test_block_kernel_jumps_replay_reference_streams(gpu, oracle):
+    model = gpu.Model("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30",
+                                        "--etaOpt", "2", "--kappaOpt", "1", "--deltaCOpt", "-1",
+                                        "--kappaMech", "0.1", "--deltaCMech", "-2", "--u", "0.2"])
+    assert model.dim == 450
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    n = 3
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ens.run(0.5, 2)
+    agree = 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.5, 2)
+        jt, jl = ens.jumps(i, 4096)
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
+    assert agree >= n - 1
+
+
+def test_block_kernel_ensemble_vs_master(gpu, oracle):
+    args = C1_ARGS[:]
+    args[args.index("--cutoff") + 1] = "150"
+    model = gpu.Model("PumpedLossyMode_C++QED", args)
+    n = 1024
+    pars = model.run_pars().mcwf
+    pars.rng = A.RNG_PHILOX
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    Dt, K = 0.5, 4
+    sums = ens.run(Dt, K)
+    master = _master_rows(oracle, model, Dt * K, Dt)
+    mean = sums[:, :model.n_avr] / n
+    for k in range(K):
+        ref = master[k + 1, 2:]
+        assert abs(mean[k, 0] - ref[0]) <= 3 * np.sqrt(max(ref[0], 1e-3) / n) + 0.01 * ref[0]
+        assert abs(mean[k, 2] - ref[2]) <= 0.02 + 0.01 * abs(ref[2])
+
+
+def test_uneven_batch_matches_each_trajectory_alone(gpu):
+    """A batch mixing dimensions 40..240 (the uneven-batch workload) gives each trajectory
+    the result it gets alone on the same random stream."""
+    rng = np.random.default_rng(7)
+    cutoffs = [20, 45, 64, 90, 120]
+    models, systems, psi0s, idx = [], [], [], []
+    for j, N in enumerate(cutoffs):
+        g = rng.uniform(1, 10)
+        eta = rng.uniform(0.5, 3)
+        args = ["--picture", "Sch", "--deltaA", "0", "--gamma", "0", "--deltaC", "0", "--kappa", "1",
+                "--eta", "%.6f" % eta, "--cutoff", str(N), "--g", "%.6f" % g]
+        m = gpu.Model("QbitMode_C++QED", args)
+        models.append(m)
+        systems.append(gpu.System(m.desc))
+    order = [0, 4, 1, 3, 2, 4, 0, 2]
+    for j in order:
+        idx.append(j)
+        psi0s.append(models[j].initial_state())
+    pars = models[0].run_pars().mcwf
+    batch = gpu.Ensemble.batch(systems, idx, psi0s, pars)
+    batch.run(0.25, 2)
+    for i, j in enumerate(order):
+        p = models[j].run_pars().mcwf
+        p.prng_stream = pars.prng_stream + i
+        alone = gpu.Ensemble(systems[j], psi0s[i], 1, p)
+        alone.run(0.25, 2)
+        a = alone.state(0, models[j].dim)
+        b = batch.state(i, models[j].dim)
+        ja, _ = alone.jumps(0)
+        jb, _ = batch.jumps(i)
+        if len(ja) == len(jb) and np.allclose(ja, jb, rtol=1e-9):
+            assert np.linalg.norm(a - b) < 1e-8, (i, j)
