@@ -136,6 +136,60 @@ def flops_model(model):
     return per_attempt, per_step, nnz
 
 
+def measured_peaks():
+    """HBM copy bandwidth and bf16 GEMM peaks measured on this pool (driver-written), else
+    the pool's earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "MEASURED_PEAKS.json"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def run_apply(model, n_states=65536, warmup=3, reps=20):
+    """Batched H/i application (cqg_system_apply_hamiltonian) on n_states device states:
+    48 bytes per state element (read psi, read+write dpsi); timed with CUDA events on the
+    launching stream."""
+    import ctypes
+
+    import torch
+
+    import cppqed_b200 as cqg
+
+    system = cqg.System(model.desc)
+    D = model.dim
+    g = torch.Generator(device="cuda").manual_seed(5)
+    psi = torch.randn(n_states, D, dtype=torch.complex128, device="cuda", generator=g)
+    dpsi = torch.zeros_like(psi)
+    stream = torch.cuda.current_stream()
+    lib = cqg.lib()
+
+    def launch():
+        rc = lib.cqg_system_apply_hamiltonian(system._h, ctypes.c_void_p(psi.data_ptr()),
+                                              ctypes.c_void_p(dpsi.data_ptr()), n_states, 0.0,
+                                              ctypes.c_void_p(stream.cuda_stream))
+        if rc:
+            raise RuntimeError(lib.cqg_last_error().decode())
+
+    for _ in range(warmup):
+        launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    bytes_per = 48.0 * n_states * D
+    peak, src = measured_peaks()
+    gbs = bytes_per / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "peak_source": src, "ms_per_launch": ms, "bytes_per_launch": bytes_per, "n_states": n_states,
+            "traffic": None, "kernel": "applyKernel (cqg_system_apply_hamiltonian)"}
+
+
 def run_ours(args, rank, world, dev):
     import numpy as np
     import torch
@@ -213,6 +267,7 @@ def run_ours(args, rank, world, dev):
     h2d = n_traj * model.dim * 16 + n_traj * (8 * 4 + 32 + 64)
     d2h = (model.n_avr + 1) * 8 + 4
 
+    apply = run_apply(model) if rank == 0 else None
     fp64_peak, fp32_peak = cqg.engine.probe_fma_peaks()
     per_attempt, per_step, nnz = flops_model(model)
     flops = float(tot[1]) * per_attempt + steps_total * per_step
@@ -227,7 +282,7 @@ def run_ours(args, rank, world, dev):
                      "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                      "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU",
                      "flops_per_attempt": per_attempt, "nnz_h": nnz},
-        "n_traj": n_traj, "model": model,
+        "n_traj": n_traj, "model": model, "apply": apply,
     }
 
 
@@ -304,7 +359,8 @@ def main():
                           "n_traj_per_gpu": n_traj, "Dt_per_step": Dt, "rng": args.rng,
                           "l2_flush": "not needed: states stay on chip; per-step HBM traffic is the state read/write",
                           "parallelism": "trajectory-sharded x%d" % world},
-               "e2e": r["e2e"], "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"],
+               "e2e": r["e2e"], "roofline": r["roofline"], "apply_roofline": r["apply"], "cpu_baseline": cpu,
+               "clocks": r["clocks"],
                "gpu_launches": 3 * args.steps,
                "counters": {"accepted_steps": r["steps_total"], "ode_attempts": r["attempts_total"],
                             "rhs_evaluations": r["rhs_total"], "kernel_ms": r["kernel_ms"]}}

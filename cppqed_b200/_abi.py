@@ -118,6 +118,7 @@ ENGINE_PROTOTYPES = {
     "cqg_system_create": (C.c_int, [C.POINTER(cqg_system_desc), C.POINTER(_P)]),
     "cqg_system_dimension": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "cqg_system_destroy": (C.c_int, [_P]),
+    "cqg_system_apply_hamiltonian": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int64, C.c_double, C.c_void_p]),
     "cqg_ensemble_create": (C.c_int, [_P, _CP, C.c_int64, C.POINTER(cqg_mcwf_pars), C.POINTER(_P)]),
     "cqg_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(C.c_int32), _CP,
                                    C.POINTER(C.c_int64), C.c_int64, C.POINTER(cqg_mcwf_pars),

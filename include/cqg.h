@@ -154,6 +154,15 @@ int cqg_system_create(const cqg_system_desc* desc, cqg_system** out);
 int cqg_system_dimension(const cqg_system* sys, int64_t* total_dim);
 int cqg_system_destroy(cqg_system* sys);
 
+/* Batched Hamiltonian::addContribution (Hamiltonian.h:38-43; the slice-wise
+ * Tridiagonal::apply of the reference, Tridiagonal.tcc:220-263):
+ *   dpsi_i += (H/i)(tau) psi_i,  i < n_states,  tau = t - t0 (interaction picture).
+ * psi and dpsi are device pointers to n_states x D complex128 states, state after state,
+ * and must not overlap.  Queued on `stream` (a cudaStream_t, NULL = default stream);
+ * returns without waiting. */
+int cqg_system_apply_hamiltonian(const cqg_system* sys, const cqg_complex* psi, cqg_complex* dpsi, int64_t n_states,
+                                 double tau, void* stream);
+
 /* ---- ensembles ----------------------------------------------------------
  * mcwf::makeEnsemble (MCWF_Trajectory.h:213-234): n_traj copies of psi0
  * (sys dimension D complex values), trajectory i seeded with stream

@@ -244,3 +244,33 @@ def test_uneven_batch_matches_each_trajectory_alone(gpu):
         jb, _ = batch.jumps(i)
         if len(ja) == len(jb) and np.allclose(ja, jb, rtol=1e-9):
             assert np.linalg.norm(a - b) < 1e-8, (i, j)
+
+
+# ---- batched H/i application (Tridiagonal::apply / Hamiltonian::addContribution) ----
+
+@pytest.mark.parametrize("picture,tau", [("Sch", 0.0), ("IP", 0.37)])
+def test_apply_hamiltonian_matches_oracle(gpu, oracle, picture, tau):
+    import ctypes
+
+    import torch
+
+    args = C2_ARGS[:]
+    args[args.index("--picture") + 1] = picture
+    args[args.index("--kappa") + 1] = "1"
+    model = gpu.Model("QbitMode_C++QED", args)
+    sysd = gpu.System(model.desc)
+    rng = np.random.default_rng(3)
+    n = 64
+    psi = rng.normal(size=(n, model.dim)) + 1j * rng.normal(size=(n, model.dim))
+    base = rng.normal(size=(n, model.dim)) + 1j * rng.normal(size=(n, model.dim))
+    d_psi = torch.from_numpy(psi).to("cuda")
+    d_out = torch.from_numpy(base).to("cuda")
+    torch.cuda.synchronize()
+    rc = gpu.lib().cqg_system_apply_hamiltonian(sysd._h, ctypes.c_void_p(d_psi.data_ptr()),
+                                                ctypes.c_void_p(d_out.data_ptr()), n, tau, None)
+    assert rc == A.CQG_OK, gpu.lib().cqg_last_error()
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy() - base
+    for i in range(0, n, 9):
+        ref = oracle.apply_hamiltonian(model, psi[i], tau)
+        assert np.linalg.norm(got[i] - ref) <= 1e-13 * np.linalg.norm(ref) + 1e-14
