@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--apply-states", type=int, default=0,
+                    help="only time the batched H/i application on this many states of the workload's system")
+    ap.add_argument("--apply-reps", type=int, default=20)
     return ap.parse_args()
 
 
@@ -147,7 +150,16 @@ def measured_peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def run_apply(model, n_states=65536, warmup=3, reps=20):
+# DRAM bytes of one launch from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum).
+# MCWF kernel: the default workload (qubit-mode 2x40, 4096 trajectories, FP64), one Dt = 1
+# launch.  Apply kernel: 65,536 states of the same system (the full 1 M-state batch is larger
+# than a capture should be); reads are exactly psi + dpsi, part of the dpsi write is still
+# in L2 when the launch ends.
+MCWF_TRAFFIC = {"workload": "qbitmode_jc_2x40", "precision": "fp64", "bytes": 6.177024e6}
+APPLY_TRAFFIC = {"n_states": 65536, "bytes": 167.799040e6 + 33.929728e6, "algorithmic_bytes": 48.0 * 65536 * 80}
+
+
+def run_apply(model, n_states=1 << 20, warmup=3, reps=20):
     """Batched H/i application (cqg_system_apply_hamiltonian) on n_states device states:
     48 bytes per state element (read psi, read+write dpsi); timed with CUDA events on the
     launching stream."""
@@ -187,7 +199,8 @@ def run_apply(model, n_states=65536, warmup=3, reps=20):
     gbs = bytes_per / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
             "peak_source": src, "ms_per_launch": ms, "bytes_per_launch": bytes_per, "n_states": n_states,
-            "traffic": None, "kernel": "applyKernel (cqg_system_apply_hamiltonian)"}
+            "traffic": APPLY_TRAFFIC if n_states == APPLY_TRAFFIC["n_states"] else None,
+            "kernel": "stagedApplyKernel (cqg_system_apply_hamiltonian)"}
 
 
 def run_ours(args, rank, world, dev):
@@ -279,7 +292,9 @@ def run_ours(args, rank, world, dev):
         "clocks": clocks, "e2e": {"value": e2e_value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": h2d,
                                   "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": MCWF_TRAFFIC["bytes"] if (args.workload, args.precision) == (
+                         MCWF_TRAFFIC["workload"], MCWF_TRAFFIC["precision"]) else None,
                      "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU",
                      "flops_per_attempt": per_attempt, "nnz_h": nnz},
         "n_traj": n_traj, "model": model, "apply": apply,
@@ -341,6 +356,12 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.apply_states:
+        import cppqed_b200 as cqg
+        script, sargs, _, _ = WORKLOADS[args.workload]
+        print(json.dumps(run_apply(cqg.Model(script, sargs), n_states=args.apply_states,
+                                   warmup=args.warmup, reps=args.apply_reps)))
+        return
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))

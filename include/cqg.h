@@ -157,8 +157,8 @@ int cqg_system_destroy(cqg_system* sys);
 /* Batched Hamiltonian::addContribution (Hamiltonian.h:38-43; the slice-wise
  * Tridiagonal::apply of the reference, Tridiagonal.tcc:220-263):
  *   dpsi_i += (H/i)(tau) psi_i,  i < n_states,  tau = t - t0 (interaction picture).
- * psi and dpsi are device pointers to n_states x D complex128 states, state after state,
- * and must not overlap.  Queued on `stream` (a cudaStream_t, NULL = default stream);
+ * psi and dpsi are 16-byte aligned device pointers to n_states x D complex128 states,
+ * state after state, and must not overlap (CQG_E_INVALID otherwise).  Queued on `stream` (a cudaStream_t, NULL = default stream);
  * returns without waiting. */
 int cqg_system_apply_hamiltonian(const cqg_system* sys, const cqg_complex* psi, cqg_complex* dpsi, int64_t n_states,
                                  double tau, void* stream);

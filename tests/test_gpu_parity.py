@@ -274,3 +274,61 @@ def test_apply_hamiltonian_matches_oracle(gpu, oracle, picture, tau):
     for i in range(0, n, 9):
         ref = oracle.apply_hamiltonian(model, psi[i], tau)
         assert np.linalg.norm(got[i] - ref) <= 1e-13 * np.linalg.norm(ref) + 1e-14
+
+
+APPLY_CASES = [
+    # (script, args, n_states): the staged kernel with several states per CTA lane set,
+    # a single state, a count that leaves a ragged last chunk, one row-lane per CTA (D=450),
+    # many states side by side (D=2), and D > 992 (element fallback)
+    ("QbitMode_C++QED", C2_ARGS, 1),
+    ("QbitMode_C++QED", C2_ARGS, 1001),
+    ("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30", "--kappaOpt", "1",
+                       "--etaOpt", "1", "--deltaCMech", "-2", "--u", "0.1"], 77),
+    ("PTLA_C++QED", [], 5000),
+    ("Optomechanics", ["--picture", "IP", "--cutoffOpt", "20", "--cutoffMech", "60", "--kappaOpt", "1",
+                       "--etaOpt", "1", "--deltaCOpt", "-1", "--deltaCMech", "-2", "--u", "0.1"], 9),
+]
+
+
+@pytest.mark.parametrize("case", range(len(APPLY_CASES)))
+@pytest.mark.parametrize("tau", [0.0, 0.29])
+def test_apply_hamiltonian_shapes(gpu, oracle, case, tau):
+    import ctypes
+
+    import torch
+
+    script, args, n = APPLY_CASES[case]
+    model = gpu.Model(script, args)
+    sysd = gpu.System(model.desc)
+    rng = np.random.default_rng(11 + case)
+    psi = rng.normal(size=(n, model.dim)) + 1j * rng.normal(size=(n, model.dim))
+    base = rng.normal(size=(n, model.dim)) + 1j * rng.normal(size=(n, model.dim))
+    d_psi = torch.from_numpy(psi).to("cuda")
+    d_out = torch.from_numpy(base).to("cuda")
+    torch.cuda.synchronize()
+    rc = gpu.lib().cqg_system_apply_hamiltonian(sysd._h, ctypes.c_void_p(d_psi.data_ptr()),
+                                                ctypes.c_void_p(d_out.data_ptr()), n, tau, None)
+    assert rc == A.CQG_OK, gpu.lib().cqg_last_error()
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy() - base
+    for i in sorted({0, n // 2, n - 1}):
+        ref = oracle.apply_hamiltonian(model, psi[i], tau)
+        assert np.linalg.norm(got[i] - ref) <= 1e-13 * np.linalg.norm(ref) + 1e-14, i
+
+
+def test_apply_hamiltonian_refuses_unaligned_pointers(gpu):
+    """The kernels move complex numbers as 16-byte vectors: a state that starts 8 bytes
+    into an allocation is refused on the host, before any launch."""
+    import ctypes
+
+    import torch
+
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    sysd = gpu.System(model.desc)
+    d = torch.zeros(2 * model.dim + 2, dtype=torch.float64, device="cuda")
+    lib = gpu.lib()
+    for dp, dq in ((8, 0), (0, 8)):
+        rc = lib.cqg_system_apply_hamiltonian(sysd._h, ctypes.c_void_p(d.data_ptr() + dp),
+                                              ctypes.c_void_p(d.data_ptr() + dq), 1, 0.0, None)
+        assert rc == A.CQG_E_INVALID
+        assert b"16-byte aligned" in lib.cqg_last_error()
