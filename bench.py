@@ -39,13 +39,35 @@ WORKLOADS = {
 }
 
 
+# Uneven batch (driven Jaynes-Cummings, qubit x mode): cutoffs uniform in [20, 120],
+# g uniform in [1, 10], eta uniform in [0.5, 3], kappa = 1, gamma = 0; one parameter draw per
+# system of UNEVEN_PER_SYSTEM trajectories (fixed seed).
+UNEVEN = {"uneven_jc_16384": (256, 64, 0.5)}  # name: (systems, trajectories per system, Dt per step)
+
+
+def uneven_models(n_systems, seed=2024):
+    import numpy as np
+
+    import cppqed_b200 as cqg
+    rng = np.random.default_rng(seed)
+    models = []
+    for _ in range(n_systems):
+        N = int(rng.integers(20, 121))
+        g = rng.uniform(1, 10)
+        eta = rng.uniform(0.5, 3)
+        args = ["--picture", "Sch", "--deltaA", "0", "--gamma", "0", "--deltaC", "0", "--kappa", "1",
+                "--eta", "%.6f" % eta, "--cutoff", str(N), "--g", "%.6f" % g]
+        models.append(cqg.Model("QbitMode_C++QED", args))
+    return models
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="qbitmode_jc_2x40", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="qbitmode_jc_2x40", choices=sorted(WORKLOADS) + sorted(UNEVEN))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
@@ -301,6 +323,121 @@ def run_ours(args, rank, world, dev):
     }
 
 
+def run_batched(args, dev):
+    """Uneven batch: every system's trajectories in one batch (one persistent launch per
+    kernel group, groups concurrent), against the plain path (one FP64 ensemble per system
+    and launch, one after another), and the FP32-state variant against FP64 on the same
+    random streams."""
+    import numpy as np
+    import torch
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    n_sys, per, Dt = UNEVEN[args.workload]
+    models = uneven_models(n_sys)
+    systems = [cqg.System(m.desc) for m in models]
+    idx = np.repeat(np.arange(n_sys), per)
+    psi0s = [models[j].initial_state() for j in idx]
+    n_traj = len(idx)
+
+    def pars_for(precision, stream=1):
+        p = models[0].run_pars().mcwf
+        p.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
+        p.precision = precision
+        p.prng_stream = stream
+        return p
+
+    def timed_batch(precision, steps, warmup, sampler=None):
+        ens = cqg.Ensemble.batch(systems, idx, psi0s, pars_for(precision))
+        for _ in range(warmup):
+            ens.run(Dt, 1)
+        c0 = ens.counters()
+        if sampler:
+            sampler.start()
+        torch.cuda.synchronize()
+        k_ms = r_ms = 0.0
+        for _ in range(steps):
+            ens.run(Dt, 1)
+            k, r = ens.last_ms()
+            k_ms += k
+            r_ms += r
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        d = ens.counters().astype(np.int64) - c0.astype(np.int64)
+        return ens, d, k_ms, r_ms, clocks
+
+    precision = A.FP64 if args.precision == "fp64" else A.FP32
+    ens, d, k_ms, r_ms, clocks = timed_batch(precision, args.steps, args.warmup, ClockSampler(dev))
+    steps_total = float(d[:, 0].sum())
+    value = steps_total / (r_ms * 1e-3)
+    plan = ens.plan()
+
+    # roofline: algorithmic FLOPs trajectory by trajectory
+    fm = [flops_model(m) for m in models]
+    flops = float(sum(d[i, 1] * fm[idx[i]][0] + d[i, 0] * fm[idx[i]][1] for i in range(n_traj)))
+    fp64_peak, fp32_peak = cqg.engine.probe_fma_peaks()
+    peak = fp64_peak if args.precision == "fp64" else fp32_peak
+    achieved = flops / (k_ms * 1e-3) / 1e12
+
+    # FP32-state variant against FP64 on the same streams after the same simulated time:
+    # difference of the batch means of every average, in units of the FP64 standard error
+    T_steps = args.warmup + args.steps
+    e64, _, _, _, _ = timed_batch(A.FP64, T_steps, 0) if precision != A.FP64 else (ens, None, 0, 0, None)
+    e32, _, _, _, _ = timed_batch(A.FP32, T_steps, 0) if precision != A.FP32 else (ens, None, 0, 0, None)
+    a64 = e64.traj_averages()[:, :models[0].n_avr]
+    a32 = e32.traj_averages()[:, :models[0].n_avr]
+    se = a64.std(axis=0, ddof=1) / np.sqrt(n_traj)
+    z = np.abs(a32.mean(axis=0) - a64.mean(axis=0)) / np.where(se > 0, se, np.inf)
+    precision_check = {"observables": models[0].key(), "max_sigma": float(z.max()),
+                       "sigma_per_observable": [float(v) for v in z], "t": T_steps * Dt,
+                       "note": "FP32-state/FP64-control batch vs the FP64 batch, same pcg64 streams"}
+    del e64, e32
+
+    # plain path: one FP64 ensemble per system and launch, one after another, same work
+    p_steps = 0
+    p_ms = 0.0
+    for j in range(n_sys):
+        e = cqg.Ensemble(systems[j], models[j].initial_state(), per, pars_for(A.FP64, 1 + j * per))
+        for _ in range(T_steps):
+            e.run(Dt, 1)
+            p_ms += e.last_ms()[1]
+        p_steps += int(e.counters()[:, 0].sum())
+        del e
+    plain_value = p_steps / (p_ms * 1e-3)
+
+    # end to end: batch created from host states, one Dt, averages read back
+    t0 = time.perf_counter()
+    e = cqg.Ensemble.batch(systems, idx, psi0s, pars_for(precision))
+    e.run(Dt, 1)
+    e2e_steps = int(e.counters()[:, 0].sum())
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    del e
+    dims = np.array([m.dim for m in models])[idx]
+    out = {"metric": "MCWF trajectory-steps/s", "value": value, "unit": "trajectory-steps/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": r_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
+           "config": {"workload": args.workload, "systems": n_sys, "trajectories_per_system": per,
+                      "n_traj": n_traj, "dim_range": [int(dims.min()), int(dims.max())], "Dt_per_step": Dt,
+                      "rng": args.rng, "kernel_groups": plan,
+                      "l2_flush": "not needed: states stay on chip"},
+           "plain_fp64": {"value": plain_value, "unit": "trajectory-steps/s",
+                          "how": "one FP64 ensemble per system and launch, sequential, same Dt intervals"},
+           "batched_vs_plain": value / plain_value,
+           "precision_check": precision_check,
+           "e2e": {"value": e2e_steps / e2e_s, "unit": "trajectory-steps/s",
+                   "h2d_bytes_per_step": int(dims.sum()) * 16, "d2h_bytes_per_step": (models[0].n_avr + 1) * 8},
+           "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved,
+                        "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                        "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU"},
+           "clocks": clocks, "gpu_launches": sum(1 for _ in plan) * args.steps + 2 * args.steps,
+           "counters": {"accepted_steps": steps_total, "ode_attempts": float(d[:, 1].sum()),
+                        "kernel_ms": k_ms}}
+    return out
+
+
 def cpu_sample(args, threads, seconds):
     """Times the oracle (the reference's serial algorithm) on a bounded sample."""
     import cppqed_b200 as cqg
@@ -356,6 +493,9 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.workload in UNEVEN:
+        print(json.dumps(run_batched(args, local)))
+        return
     if args.apply_states:
         import cppqed_b200 as cqg
         script, sargs, _, _ = WORKLOADS[args.workload]

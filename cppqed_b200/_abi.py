@@ -88,6 +88,8 @@ class cqg_mcwf_pars(C.Structure):
         ("noise", C.c_int32),
         ("precision", C.c_int32),
         ("max_attempts", C.c_int32),
+        ("autotune", C.c_int32),
+        ("cta_threads", C.c_int32),
     ]
 
 
@@ -137,6 +139,7 @@ ENGINE_PROTOTYPES = {
                                          C.POINTER(C.c_int32)]),
     "cqg_ensemble_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
+    "cqg_ensemble_plan": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
     "cqg_ensemble_destroy": (C.c_int, [_P]),
     "cqg_system_averages_noalloc": (C.c_int, [_P, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),

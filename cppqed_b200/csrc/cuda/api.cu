@@ -6,6 +6,9 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -65,10 +68,25 @@ struct cqg_system {
   }
 };
 
+// One persistent launch per run call: the trajectories of one kernel shape, a segment of
+// the ensemble's order array, on their own stream.
+struct KernelGroup {
+  int kind = 0;     // 0: warp per trajectory, 1: CTA per trajectory
+  int E = 0;        // warp kind: rows per lane
+  int smax = 0;     // off-diagonal slots per row (max over the group's systems)
+  int Dmax = 0;
+  int threads = 0;  // CTA size
+  int64_t first = 0, count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  void* scratch = nullptr;  // block kind: per-CTA stage vectors
+  size_t scratchBytes = 0;
+};
+
 struct cqg_ensemble {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evRun0 = nullptr, evRun1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evRun0 = nullptr, evRun1 = nullptr, evFork = nullptr;
   float lastMs = 0, lastRunMs = 0;
   int64_t nTraj = 0;
   int nAvrMax = 0, Dmax = 0, Smax = 0;
@@ -76,23 +94,26 @@ struct cqg_ensemble {
   std::vector<const cqg_system*> systems;
   std::vector<int> sysIdx;
   std::vector<long long> psiOff;
+  std::vector<KernelGroup> groups;
   size_t elemBytes = 16;
   // device buffers
   void* dmem = nullptr;
   dev::TrajDev td{};
   dev::SysDev* dSystems = nullptr;
-  int* dQueue = nullptr;
+  int* dQueue = nullptr;  // one work-queue counter per group
   int* dOrder = nullptr;
   unsigned* dStatusOr = nullptr;
   double* dAvr = nullptr;
   size_t avrCap = 0;
   double* dSums = nullptr;
   size_t sumsCap = 0;
-  void* dBlockScratch = nullptr;  // per-CTA stage vectors of the block kernel
-  size_t blockScratchBytes = 0;
   int jumpCap = 64;
   ~cqg_ensemble() {
-    if (dBlockScratch) cudaFree(dBlockScratch);
+    for (auto& g : groups) {
+      if (g.scratch) cudaFree(g.scratch);
+      if (g.done) cudaEventDestroy(g.done);
+      if (g.stream) cudaStreamDestroy(g.stream);
+    }
     if (dAvr) cudaFree(dAvr);
     if (dSums) cudaFree(dSums);
     if (dmem) cudaFree(dmem);
@@ -100,6 +121,7 @@ struct cqg_ensemble {
     if (ev1) cudaEventDestroy(ev1);
     if (evRun0) cudaEventDestroy(evRun0);
     if (evRun1) cudaEventDestroy(evRun1);
+    if (evFork) cudaEventDestroy(evFork);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -271,6 +293,13 @@ namespace {
 
 // the warp kernel holds up to 4 rows per lane
 constexpr int kWarpKernelMaxD = 128;
+// kernel groups: warp kernel with E = 1..4 rows per lane, and the block kernel
+constexpr int kMaxGroups = 5;
+
+int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
+
+int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
+                 const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars);
 
 KernelFn pickKernel(bool fp64, int E, int SMAX) {
   if (fp64)
@@ -339,6 +368,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   ck(cudaEventCreate(&e->ev1), "cudaEventCreate");
   ck(cudaEventCreate(&e->evRun0), "cudaEventCreate");
   ck(cudaEventCreate(&e->evRun1), "cudaEventCreate");
+  ck(cudaEventCreateWithFlags(&e->evFork, cudaEventDisableTiming), "cudaEventCreate");
   e->elemBytes = pars->precision == CQG_FP64 ? 16 : 8;
 
   e->sysIdx.resize(nTraj);
@@ -358,7 +388,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
                oT = A.add(nTraj * 8), oT0 = A.add(nTraj * 8), oTry = A.add(nTraj * 8), oDid = A.add(nTraj * 8),
                oRng = A.add(nTraj * 32), oCnt = A.add(nTraj * 64), oMax = A.add(nTraj * 24), oSt = A.add(nTraj * 4),
                oJT = A.add(nTraj * e->jumpCap * 8), oJL = A.add(nTraj * e->jumpCap * 4), oJN = A.add(nTraj * 8),
-               oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(16), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
+               oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(kMaxGroups * sizeof(int)), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
   ck(cudaMalloc(&e->dmem, A.total), "cudaMalloc(ensemble)");
   ck(cudaMemset(e->dmem, 0, A.total), "cudaMemset");
   char* b = static_cast<char*>(e->dmem);
@@ -437,16 +467,99 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   e->dQueue = reinterpret_cast<int*>(b + oQ);
   e->dOrder = reinterpret_cast<int*>(b + oOrd);
   e->dStatusOr = reinterpret_cast<unsigned*>(b + oSOr);
-  // longest trajectories first (dimension as the cost proxy) for the work queue
+  // kernel groups: CTA-per-trajectory for D > 128, else warp-per-trajectory by rows per
+  // lane; heavier groups first, and inside a group the longest trajectories first
+  // (dimension as the cost proxy) for its work queue
+  auto groupKey = [&](int64_t i) {
+    const int D = int(systems[e->sysIdx[i]]->L.D);
+    return D <= kWarpKernelMaxD ? (D + 31) / 32 : kMaxGroups;
+  };
   std::vector<int> order(nTraj);
   std::iota(order.begin(), order.end(), 0);
-  if (nSys > 1)
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-      return systems[e->sysIdx[a]]->L.D > systems[e->sysIdx[c]]->L.D;
-    });
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    const int ka = groupKey(a), kc = groupKey(c);
+    if (ka != kc) return ka > kc;
+    return systems[e->sysIdx[a]]->L.D > systems[e->sysIdx[c]]->L.D;
+  });
+  for (int64_t k = 0; k < nTraj;) {
+    KernelGroup g;
+    const int key = groupKey(order[k]);
+    g.kind = key == kMaxGroups ? 1 : 0;
+    g.E = g.kind ? 0 : key;
+    g.first = k;
+    for (; k < nTraj && groupKey(order[k]) == key; ++k) {
+      const cqg_system* s = systems[e->sysIdx[order[k]]];
+      g.Dmax = std::max<int>(g.Dmax, int(s->L.D));
+      g.smax = std::max(g.smax, s->sd.S);
+    }
+    g.count = k - g.first;
+    e->groups.push_back(g);
+  }
   upload(b, oOrd, order);
+  for (auto& g : e->groups) {
+    if (e->groups.size() > 1) {
+      ck(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+      ck(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    g.threads = pars->cta_threads > 0 ? pars->cta_threads : defaultThreads(g);
+    if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 256 : 128))
+      return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 256");
+  }
+  if (pars->autotune && pars->cta_threads <= 0)
+    for (size_t gi = 0; gi < e->groups.size(); ++gi)
+      e->groups[gi].threads = tunedThreads(*e, gi, systems, nSys, psi0s, psi0Off, *pars);
   *out = e.release();
   return CQG_OK;
+}
+
+// One persistent launch of a kernel group on stream st.
+void launchGroup(cqg_ensemble& e, KernelGroup& g, dev::RunArgs ra, int nSM, cudaStream_t st) {
+  const bool fp64 = e.pars.precision == CQG_FP64;
+  dev::TrajDev tdArg = e.td;
+  if (g.kind == 0) {
+    KernelFn fn = pickKernel(fp64, g.E, g.smax);
+    const int warps = g.threads / 32;
+    const size_t smem = size_t(warps) * 3 * 32 * g.E * e.elemBytes + size_t(warps) * sizeof(dev::WarpScratch);
+    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+       "cudaFuncSetAttribute");
+    int perSM = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), g.threads, smem),
+       "occupancy");
+    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (g.count + warps - 1) / warps));
+    grid = std::max(grid, 1);
+    void* args[] = {&tdArg, &ra};
+    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(g.threads), args, smem, st),
+       "kernel launch");
+  } else {
+    // one CTA per trajectory: stage vectors in shared memory, stage derivatives in a
+    // per-CTA scratch slab
+    dev::BlockKernelFn fn = dev::pick_block(fp64);
+    int smemD = g.Dmax;
+    const size_t smem = 2 * size_t(smemD) * e.elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+       "cudaFuncSetAttribute");
+    int perSM = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), g.threads, smem),
+       "occupancy");
+    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, g.count));
+    grid = std::max(grid, 1);
+    dev::BlockScratch bsc;
+    bsc.stride = (g.Dmax + 31) / 32 * 32;
+    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * e.elemBytes;
+    if (need > g.scratchBytes) {
+      if (g.scratch) {
+        ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        cudaFree(g.scratch);
+      }
+      g.scratch = nullptr;
+      ck(cudaMalloc(&g.scratch, need), "cudaMalloc(block scratch)");
+      g.scratchBytes = need;
+    }
+    bsc.base = g.scratch;
+    void* args[] = {&tdArg, &ra, &bsc, &smemD};
+    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(g.threads), args, smem, st),
+       "kernel launch");
+  }
 }
 
 int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
@@ -468,12 +581,10 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   }
   ck(cudaEventRecord(e->evRun0, e->stream), "cudaEventRecord");
   ck(cudaMemsetAsync(e->dAvr, 0, need * sizeof(double), e->stream), "cudaMemsetAsync");
-  ck(cudaMemsetAsync(e->dQueue, 0, sizeof(int), e->stream), "cudaMemsetAsync");
+  ck(cudaMemsetAsync(e->dQueue, 0, kMaxGroups * sizeof(int), e->stream), "cudaMemsetAsync");
   ck(cudaMemsetAsync(e->dStatusOr, 0, sizeof(unsigned), e->stream), "cudaMemsetAsync");
   ra.avrOut = e->dAvr;
   ra.nAvrStride = nAvr;
-  ra.queue = e->dQueue;
-  ra.order = e->systems.size() > 1 ? e->dOrder : nullptr;
   ra.absSlot = e->pars.eps_rel;  // make_controlled(epsRel, epsAbs, ...) (ODE.h:205)
   ra.relSlot = e->pars.eps_abs;
   ra.dpLimit = e->pars.dp_limit;
@@ -487,54 +598,21 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
 
   int nSM = 0;
   ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e->device), "attribute");
-  if (e->Dmax <= kWarpKernelMaxD) {
-    const int E = (e->Dmax + 31) / 32;  // rows per lane, 1..4
-    KernelFn fn = pickKernel(e->pars.precision == CQG_FP64, E, e->Smax);
-    const int threads = 128;
-    const size_t smem =
-        size_t(threads / 32) * 3 * 32 * E * e->elemBytes + size_t(threads / 32) * sizeof(dev::WarpScratch);
-    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-       "cudaFuncSetAttribute");
-    int perSM = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem),
-       "occupancy");
-    const int64_t warpsNeeded = e->nTraj;
-    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (warpsNeeded + 3) / 4));
-    grid = std::max(grid, 1);
-    ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
-    dev::TrajDev tdArg = e->td;
-    void* args[] = {&tdArg, &ra};
-    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(threads), args, smem, e->stream),
-       "kernel launch");
-  } else {
-    // one CTA per trajectory: stage vectors in shared memory, stage derivatives in a
-    // per-CTA scratch slab
-    dev::BlockKernelFn fn = dev::pick_block(e->pars.precision == CQG_FP64);
-    const int threads = 256;
-    int smemD = e->Dmax;
-    const size_t smem = 2 * size_t(smemD) * e->elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
-    ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-       "cudaFuncSetAttribute");
-    int perSM = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, reinterpret_cast<const void*>(fn), threads, smem),
-       "occupancy");
-    int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, e->nTraj));
-    grid = std::max(grid, 1);
-    dev::BlockScratch bsc;
-    bsc.stride = (e->Dmax + 31) / 32 * 32;
-    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * e->elemBytes;
-    if (need > e->blockScratchBytes) {
-      if (e->dBlockScratch) cudaFree(e->dBlockScratch);
-      e->dBlockScratch = nullptr;
-      ck(cudaMalloc(&e->dBlockScratch, need), "cudaMalloc(block scratch)");
-      e->blockScratchBytes = need;
+  ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
+  const bool fork = e->groups.size() > 1;
+  if (fork) ck(cudaEventRecord(e->evFork, e->stream), "cudaEventRecord");
+  for (size_t gi = 0; gi < e->groups.size(); ++gi) {
+    KernelGroup& g = e->groups[gi];
+    cudaStream_t st = fork ? g.stream : e->stream;
+    if (fork) ck(cudaStreamWaitEvent(st, e->evFork, 0), "cudaStreamWaitEvent");
+    ra.order = e->dOrder + g.first;
+    ra.nTasks = int(g.count);
+    ra.queue = e->dQueue + gi;
+    launchGroup(*e, g, ra, nSM, st);
+    if (fork) {
+      ck(cudaEventRecord(g.done, st), "cudaEventRecord");
+      ck(cudaStreamWaitEvent(e->stream, g.done, 0), "cudaStreamWaitEvent");
     }
-    bsc.base = e->dBlockScratch;
-    ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
-    dev::TrajDev tdArg = e->td;
-    void* args[] = {&tdArg, &ra, &bsc, &smemD};
-    ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(threads), args, smem, e->stream),
-       "kernel launch");
   }
   ck(cudaEventRecord(e->ev1, e->stream), "cudaEventRecord");
   if (nAvr > 0 && nOut > 0) {
@@ -558,6 +636,78 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   if (bits & 3u) return fail(CQG_E_NONFINITE, "a trajectory produced a non-finite norm or rate");
   if (bits & 12u) return fail(CQG_E_STALLED, "a trajectory exhausted its step-size or attempt budget");
   return CQG_OK;
+}
+
+// Autotuner of the CTA size of a kernel group: the candidates are timed on a sample of
+// the group's trajectories (a scratch ensemble from the same initial states, so the
+// ensemble itself is not advanced) over a fixed number of MCWF steps each, and the fastest
+// is kept.  Results are cached per (device, precision, kernel kind, rows per lane, slot
+// bound, largest dimension) for the life of the process.
+std::vector<int> threadCandidates(const KernelGroup& g) {
+  std::vector<int> c;
+  if (g.kind == 0) return {64, 128};
+  for (int q = 1; q <= 4; ++q) {  // rows per thread
+    const int t = std::min(256, std::max(64, ((g.Dmax + q - 1) / q + 31) / 32 * 32));
+    if (std::find(c.begin(), c.end(), t) == c.end()) c.push_back(t);
+  }
+  if (std::find(c.begin(), c.end(), 256) == c.end()) c.push_back(256);
+  return c;
+}
+
+int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
+                 const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+  const KernelGroup& g = e.groups[gi];
+  const auto key = std::make_tuple(e.device, pars.precision, g.kind, g.E, g.smax, g.Dmax);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  const std::vector<int> cands = threadCandidates(g);
+  int nSM = 0;
+  ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e.device), "attribute");
+  // enough trajectories to fill the device a couple of times over
+  const int64_t want = g.kind ? int64_t(nSM) * 4 : int64_t(nSM) * 16;
+  if (g.count < want / 2) return defaultThreads(g);  // too small to time; nothing cached
+  const int64_t n = std::min<int64_t>(g.count, want);
+  std::vector<int> order(e.nTraj);
+  ck(cudaMemcpy(order.data(), e.dOrder, order.size() * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(order)");
+  std::vector<int32_t> sIdx(n);
+  std::vector<int64_t> sOff(n);
+  for (int64_t k = 0; k < n; ++k) {
+    const int ti = order[g.first + k];
+    sIdx[k] = e.sysIdx[ti];
+    sOff[k] = psi0Off ? psi0Off[ti] : 0;
+  }
+  cqg_mcwf_pars tp = pars;
+  tp.autotune = 0;
+  tp.cta_threads = cands[0];
+  cqg_ensemble* tmp = nullptr;
+  if (createEnsemble(systems, nSys, sIdx.data(), psi0s, psi0Off ? sOff.data() : nullptr, n, &tp, &tmp) != CQG_OK)
+    return defaultThreads(g);
+  std::unique_ptr<cqg_ensemble> hold(tmp);
+  if (tmp->groups.size() != 1) return defaultThreads(g);
+  dev::RunArgs ra{};
+  ra.mode = dev::RUN_STEPS;
+  ra.nIntervals = 1;
+  ra.T = 1e300;
+  int best = defaultThreads(g);
+  float bestMs = 0;
+  for (int pass = 0; pass < 2; ++pass)  // pass 0 warms up every candidate
+    for (int c : cands) {
+      tmp->groups[0].threads = c;
+      ra.nSteps = pass ? 12 : 2;
+      if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
+      if (pass && (bestMs == 0 || tmp->lastMs < bestMs)) {
+        bestMs = tmp->lastMs;
+        best = c;
+      }
+    }
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = best;
+  return best;
 }
 
 }  // namespace
@@ -714,6 +864,21 @@ int cqg_ensemble_traj_averages(cqg_ensemble* ens, double* out) {
        "cudaMemcpy");
     return CQG_OK;
   });
+}
+
+int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap) {
+  if (!ens || !n_groups || (cap > 0 && !plan)) return fail(CQG_E_INVALID, "cqg_ensemble_plan: null argument");
+  *n_groups = int32_t(ens->groups.size());
+  for (int32_t g = 0; g < std::min<int32_t>(cap, *n_groups); ++g) {
+    const KernelGroup& k = ens->groups[g];
+    int32_t* o = plan + 5 * g;
+    o[0] = k.kind;
+    o[1] = k.E;
+    o[2] = k.smax;
+    o[3] = k.threads;
+    o[4] = int32_t(k.count);
+  }
+  return CQG_OK;
 }
 
 int cqg_ensemble_size(const cqg_ensemble* ens, int64_t* n_traj, int32_t* n_avr) {

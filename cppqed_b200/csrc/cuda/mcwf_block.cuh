@@ -473,8 +473,8 @@ __global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, B
     __syncthreads();
     if (threadIdx.x == 0) task = atomicAdd(ra.queue, 1);
     __syncthreads();
-    if (task >= td.nTraj) return;
-    const int ti = ra.order ? ra.order[task] : task;
+    if (task >= ra.nTasks) return;
+    const int ti = ra.order[task];
     const SysDev* s = td.systems + td.sysIdx[ti];
     BlockWorker<R> w{s, ra};
     w.D = s->D;

@@ -205,7 +205,8 @@ struct RunArgs {
   double* avrOut;   // [nOut][nTraj][nAvrStride] or null
   int nAvrStride;
   int* queue;
-  const int* order;
+  const int* order;  // the launch's trajectories (a segment of the ensemble's order)
+  int nTasks;        // how many
 };
 
 // Cash-Karp tableau (published coefficients)
@@ -758,8 +759,8 @@ __global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td
     int task = 0;
     if (lane == 0) task = atomicAdd(ra.queue, 1);
     task = __shfl_sync(FULL, task, 0);
-    if (task >= td.nTraj) return;
-    const int ti = ra.order ? ra.order[task] : task;
+    if (task >= ra.nTasks) return;
+    const int ti = ra.order[task];
     Worker<R, E, SMAX> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws);
     w.run(td, ti);
   }

@@ -37,6 +37,8 @@ void cqg_mcwf_pars_default(cqg_mcwf_pars* p) {
   p->noise = 1;
   p->precision = CQG_FP64;
   p->max_attempts = 0;
+  p->autotune = 1;
+  p->cta_threads = 0;
 }
 
 }  // extern "C"

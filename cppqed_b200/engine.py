@@ -253,6 +253,15 @@ class Ensemble:
         check(lib().cqg_ensemble_last_kernel_ms(self._h, C.byref(k), C.byref(r)))
         return k.value, r.value
 
+    def plan(self):
+        """Kernel groups: list of dicts (kind, E, smax, threads, count)."""
+        n = C.c_int32()
+        check(lib().cqg_ensemble_plan(self._h, C.byref(n), None, 0))
+        buf = (C.c_int32 * (5 * max(n.value, 1)))()
+        check(lib().cqg_ensemble_plan(self._h, C.byref(n), buf, n.value))
+        keys = ("kind", "E", "smax", "threads", "count")
+        return [dict(zip(keys, buf[5 * g:5 * g + 5])) for g in range(n.value)]
+
 
 def probe_fma_peaks():
     """Measured FP64 and FP32 FMA throughput (TFLOP/s) of the current device."""

@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 #define CQG_MAX_RANK 8
-#define CQG_ABI_VERSION 1
+#define CQG_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define CQG_OK 0
@@ -135,6 +135,10 @@ typedef struct cqg_mcwf_pars {
   int32_t noise;               /* --noise: 0 switches the Liouvillean off (Structure.h:97-103) */
   int32_t precision;           /* CQG_FP64 / CQG_FP32 */
   int32_t max_attempts;        /* bounded ODE retries per step (0: default 100000) */
+  int32_t autotune;            /* 1: time the candidate CTA shapes of each kernel group on a
+                                  sample of its trajectories at creation and keep the fastest
+                                  (cached per shape class and device); 0: fixed defaults */
+  int32_t cta_threads;         /* > 0: force this CTA size on every group (no tuning) */
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);
@@ -228,6 +232,14 @@ int cqg_ensemble_status(const cqg_ensemble* ens, uint32_t* bits);
  * ensemble's stream): the MCWF kernel alone, and every device operation of the
  * call (initialisation, kernel, reduction, read-back).  Either pointer may be NULL. */
 int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, double* run_ms);
+
+/* Launch plan of an ensemble (no reference counterpart: the reference runs its
+ * trajectories one after another).  Trajectories are grouped by kernel shape, each group
+ * one persistent launch per run call, the groups on concurrent streams.  Writes the number
+ * of groups to *n_groups and, for the first min(n_groups, cap) groups, five int32 each to
+ * plan: kind (0 = warp per trajectory, 1 = CTA per trajectory), rows per lane E (warp
+ * kind), off-diagonal slot bound, CTA threads, trajectories in the group. */
+int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap);
 
 /* Measured FMA throughput of the current device (TFLOP/s, 2 flops per FMA) for
  * FP64 and FP32 CUDA cores: the denominator of the kernels' roofline and an

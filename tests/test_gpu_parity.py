@@ -332,3 +332,72 @@ def test_apply_hamiltonian_refuses_unaligned_pointers(gpu):
                                               ctypes.c_void_p(d.data_ptr() + dq), 1, 0.0, None)
         assert rc == A.CQG_E_INVALID
         assert b"16-byte aligned" in lib.cqg_last_error()
+
+
+# ---- kernel groups and CTA shapes ----
+
+def _jc_model(gpu, N, g=2.0, eta=1.5, gamma="0"):
+    args = ["--picture", "Sch", "--deltaA", "0", "--gamma", gamma, "--deltaC", "0", "--kappa", "1",
+            "--eta", "%.6f" % eta, "--cutoff", str(N), "--g", "%.6f" % g]
+    return gpu.Model("QbitMode_C++QED", args)
+
+
+def test_batch_plan_groups_by_kernel_shape(gpu):
+    """Dimensions 40..240 split into CTA-per-trajectory (D > 128) and warp groups by rows
+    per lane, heaviest first; every trajectory is in exactly one group."""
+    cutoffs = [20, 45, 64, 90, 120]
+    models = [_jc_model(gpu, N) for N in cutoffs]
+    systems = [gpu.System(m.desc) for m in models]
+    idx = [0, 4, 1, 3, 2, 4, 0, 2, 3, 3]
+    pars = models[0].run_pars().mcwf
+    batch = gpu.Ensemble.batch(systems, idx, [models[j].initial_state() for j in idx], pars)
+    plan = batch.plan()
+    assert [(p["kind"], p["E"]) for p in plan] == [(1, 0), (0, 4), (0, 3), (0, 2)]
+    assert [p["count"] for p in plan] == [5, 2, 1, 2]
+    assert plan[0]["threads"] == 256 and all(p["threads"] == 128 for p in plan[1:])
+
+
+def test_cta_shape_does_not_change_warp_trajectories(gpu):
+    """The warp kernel advances each trajectory inside one warp, so the CTA size (forced
+    or autotuned) leaves every state bit-identical."""
+    model = _jc_model(gpu, 40, gamma="0.5")
+    sysd = gpu.System(model.desc)
+    n = 2400  # large enough for the autotuner to time the candidates
+    states = []
+    for autotune, cta in ((0, 128), (0, 64), (1, 0)):
+        pars = model.run_pars().mcwf
+        pars.autotune = autotune
+        pars.cta_threads = cta
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        plan = ens.plan()
+        assert len(plan) == 1 and plan[0]["kind"] == 0 and plan[0]["threads"] in (64, 128)
+        if cta:
+            assert plan[0]["threads"] == cta
+        ens.run(0.2, 1)
+        states.append(np.stack([ens.state(i, model.dim) for i in range(0, n, 97)]))
+    assert np.array_equal(states[0], states[1]) and np.array_equal(states[0], states[2])
+
+
+def test_block_kernel_cta_shapes_agree(gpu):
+    """The CTA-per-trajectory kernel with 64, 160 and 256 threads (one to three rows per
+    thread at D = 450) follows the same trajectories up to the summation order."""
+    model = gpu.Model("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30",
+                                        "--etaOpt", "2", "--kappaOpt", "1", "--deltaCOpt", "-1",
+                                        "--kappaMech", "0.1", "--deltaCMech", "-2", "--u", "0.2"])
+    sysd = gpu.System(model.desc)
+    n = 6
+    runs = []
+    for cta in (256, 160, 64):
+        pars = model.run_pars().mcwf
+        pars.cta_threads = cta
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        assert ens.plan()[0]["threads"] == cta
+        ens.run(0.3, 1)
+        runs.append([(ens.state(i, model.dim), ens.jumps(i)[0]) for i in range(n)])
+    for other in runs[1:]:
+        agree = 0
+        for (a, ja), (b, jb) in zip(runs[0], other):
+            if len(ja) == len(jb) and np.allclose(ja, jb, rtol=1e-9):
+                agree += 1
+                assert np.linalg.norm(a - b) < 1e-9
+        assert agree >= n - 1
