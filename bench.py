@@ -44,6 +44,52 @@ WORKLOADS = {
 # system of UNEVEN_PER_SYSTEM trajectories (fixed seed).
 UNEVEN = {"uneven_jc_16384": (256, 64, 0.5)}  # name: (systems, trajectories per system, Dt per step)
 
+# Serving: Poisson arrivals (mean SERVING["rate"] requests/s, fixed seed) of ensemble requests
+# of 64-1024 trajectories over a library of systems: pumped lossy mode, cutoff 20-200;
+# qubit-mode 2 x (10-100); the 6-qubit chain with local decay (dim 64); optomechanics 15 x 30.
+# Every request evolves to T with output interval Dt.
+SERVING = {"serving_poisson_200": {"rate": 200.0, "requests": 400, "T": 0.5, "Dt": 0.125, "seed": 77}}
+
+
+def serving_library():
+    """(kind, model) pairs: cutoffs on a grid of 10, so a service keeps ~30 systems."""
+    import cppqed_b200 as cqg
+    lib = []
+    for N in range(20, 201, 10):
+        lib.append(("mode", cqg.Model("PumpedLossyMode_C++QED",
+                                      ["--picture", "Sch", "--deltaC", "-1", "--eta", "2", "--kappa", "1",
+                                       "--cutoff", str(N), "--no_quadratures"])))
+    for N in range(10, 101, 10):
+        lib.append(("qubit-mode", cqg.Model("QbitMode_C++QED",
+                                            ["--picture", "Sch", "--deltaA", "0", "--gamma", "0.5", "--deltaC",
+                                             "0", "--kappa", "1", "--eta", "1.5", "--cutoff", str(N), "--g", "2"])))
+    lib.append(("chain", cqg.Model("QbitChain", ["--nQbit", "6", "--deltaA", "0", "--gamma", "0.2", "--etat", "0.5",
+                                                  "--u", "1"])))
+    lib.append(("optomechanics", cqg.Model("Optomechanics",
+                                           ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30",
+                                            "--etaOpt", "2", "--kappaOpt", "1", "--deltaCOpt", "-1",
+                                            "--kappaMech", "0.1", "--deltaCMech", "-2", "--u", "0.2"])))
+    return lib
+
+
+def serving_requests(cfg, lib):
+    """Seeded request list: (arrival s, library index, trajectories, prng stream)."""
+    import numpy as np
+    rng = np.random.default_rng(cfg["seed"])
+    kinds = sorted({k for k, _ in lib})
+    by_kind = {k: [i for i, (kk, _) in enumerate(lib) if kk == k] for k in kinds}
+    t = 0.0
+    out = []
+    stream = 1
+    for _ in range(cfg["requests"]):
+        t += rng.exponential(1.0 / cfg["rate"])
+        k = kinds[int(rng.integers(len(kinds)))]
+        j = by_kind[k][int(rng.integers(len(by_kind[k])))]
+        n = int(rng.integers(64, 1025))
+        out.append((t, j, n, stream))
+        stream += n
+    return out
+
 
 def uneven_models(n_systems, seed=2024):
     import numpy as np
@@ -67,7 +113,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="qbitmode_jc_2x40", choices=sorted(WORKLOADS) + sorted(UNEVEN))
+    ap.add_argument("--workload", default="qbitmode_jc_2x40",
+                    choices=sorted(WORKLOADS) + sorted(UNEVEN) + sorted(SERVING))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
@@ -438,6 +485,100 @@ def run_batched(args, dev):
     return out
 
 
+def run_serving(args, dev):
+    """Requests arrive on a seeded Poisson schedule in real time; the server admits them
+    between rounds (continuous batching) and each is timed from its scheduled arrival to
+    the end of the round that retires it.  The plain path serves the same requests one at a
+    time as FP64 ensembles, one launch per output interval."""
+    import numpy as np
+    import torch
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    cfg = SERVING[args.workload]
+    lib = serving_library()
+    systems = [cqg.System(m.desc) for _, m in lib]
+    reqs = serving_requests(cfg, lib)
+    pars = lib[0][1].run_pars().mcwf
+    pars.precision = A.FP64 if args.precision == "fp64" else A.FP32
+    pars.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
+
+    def serve(requests, sampler=None):
+        srv = cqg.Server(pars, hbm_budget_bytes=16 << 30, max_trajectories=1 << 17)
+        psi0 = [m.initial_state() for _, m in lib]
+        arrival = {}
+        done = {}
+        k = 0
+        if sampler:
+            sampler.start()
+        t0 = time.perf_counter()
+        while len(done) < len(requests):
+            now = time.perf_counter() - t0
+            while k < len(requests) and requests[k][0] <= now:
+                a, j, n, stream = requests[k]
+                rid = srv.submit(systems[j], psi0[j], n, cfg["T"], cfg["Dt"], stream)
+                arrival[rid] = (a, k)
+                k += 1
+            active, waiting = srv.round()
+            now = time.perf_counter() - t0
+            for rid in srv.completed():
+                rows, steps, _, status = srv.result(rid)
+                done[rid] = (now - arrival[rid][0], steps, status)
+            if active == 0 and waiting == 0 and k < len(requests):
+                time.sleep(max(0.0, requests[k][0] - (time.perf_counter() - t0)))
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop() if sampler else None
+        steps, kernel_ms, rounds = srv.stats()
+        lat = np.array([v[0] for v in done.values()]) * 1e3
+        bad = sum(1 for v in done.values() if v[2])
+        return {"wall_s": wall, "steps": steps, "kernel_ms": kernel_ms, "rounds": rounds, "lat_ms": lat,
+                "failed": bad, "clocks": clocks}
+
+    # warm-up: a few requests through a fresh server
+    serve([(0.0,) + r[1:] for r in reqs[:max(3, args.warmup)]])
+    res = serve(reqs, ClockSampler(dev))
+    lat = res["lat_ms"]
+
+    # plain: one FP64 ensemble per request, one launch per output interval, sequentially
+    plain_steps = 0
+    plain_ms = 0.0
+    p64 = lib[0][1].run_pars().mcwf
+    p64.precision = A.FP64
+    nInt = int(round(cfg["T"] / cfg["Dt"]))
+    for (a, j, n, stream) in reqs:
+        p64.prng_stream = stream
+        e = cqg.Ensemble(systems[j], lib[j][1].initial_state(), n, p64)
+        e.run(cfg["Dt"], 1)  # the first run of an ensemble allocates its output buffers
+        plain_ms += e.last_ms()[0]
+        for _ in range(nInt - 1):
+            e.run(cfg["Dt"], 1)
+            plain_ms += e.last_ms()[0]
+        plain_steps += int(e.counters()[:, 0].sum())
+        del e
+    plain_value = plain_steps / (plain_ms * 1e-3)
+    value = res["steps"] / res["wall_s"]
+    device_value = res["steps"] / (res["kernel_ms"] * 1e-3)
+    offered = sum(r[2] for r in reqs)
+    return {"metric": "MCWF trajectory-steps/s", "value": value, "unit": "trajectory-steps/s", "n_gpus": 1,
+            "steps": len(reqs), "warmup": max(3, args.warmup), "ms_per_step": res["wall_s"] * 1e3 / len(reqs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
+            "config": {"workload": args.workload, "arrival_rate_per_s": cfg["rate"], "requests": len(reqs),
+                       "trajectories": offered, "T": cfg["T"], "Dt": cfg["Dt"], "library_systems": len(lib),
+                       "hbm_budget_bytes": 16 << 30, "step": "one request (arrival to retirement)"},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max()), "mean": float(lat.mean())},
+            "device_value": device_value, "rounds": res["rounds"], "failed_requests": res["failed"],
+            "plain_fp64": {"value": plain_value, "unit": "trajectory-steps/s",
+                           "how": "every request as one FP64 ensemble, one launch per Dt, sequential; "
+                                  "device time of the MCWF launches"},
+            "served_device_vs_plain": device_value / plain_value,
+            "clocks": res["clocks"], "gpu_launches": None,
+            "e2e": {"value": value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None}}
+
+
 def cpu_sample(args, threads, seconds):
     """Times the oracle (the reference's serial algorithm) on a bounded sample."""
     import cppqed_b200 as cqg
@@ -495,6 +636,9 @@ def main():
     torch.cuda.set_device(local)
     if args.workload in UNEVEN:
         print(json.dumps(run_batched(args, local)))
+        return
+    if args.workload in SERVING:
+        print(json.dumps(run_serving(args, local)))
         return
     if args.apply_states:
         import cppqed_b200 as cqg

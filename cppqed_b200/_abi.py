@@ -93,6 +93,17 @@ class cqg_mcwf_pars(C.Structure):
     ]
 
 
+class cqg_server_pars(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64),
+        ("max_trajectories", C.c_int32),
+        ("max_systems", C.c_int32),
+        ("max_averages", C.c_int32),
+        ("reserved", C.c_int32),
+        ("mcwf", cqg_mcwf_pars),
+    ]
+
+
 class cqg_run_pars(C.Structure):
     _fields_ = [
         ("T", C.c_double),
@@ -141,6 +152,16 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
     "cqg_ensemble_plan": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
+    "cqg_server_pars_default": (None, [C.POINTER(cqg_server_pars)]),
+    "cqg_server_create": (C.c_int, [C.POINTER(cqg_server_pars), C.POINTER(_P)]),
+    "cqg_server_submit": (C.c_int, [_P, _P, _CP, C.c_int64, C.c_double, C.c_double, C.c_uint64,
+                                    C.POINTER(C.c_int64)]),
+    "cqg_server_round": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "cqg_server_completed": (C.c_int, [_P, C.POINTER(C.c_int64), C.c_int32, C.POINTER(C.c_int32)]),
+    "cqg_server_result": (C.c_int, [_P, C.c_int64, _DP, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_uint64), _DP, C.POINTER(C.c_uint32)]),
+    "cqg_server_stats": (C.c_int, [_P, C.POINTER(C.c_uint64), _DP, C.POINTER(C.c_int64)]),
+    "cqg_server_destroy": (C.c_int, [_P]),
     "cqg_ensemble_destroy": (C.c_int, [_P]),
     "cqg_system_averages_noalloc": (C.c_int, [_P, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "cqg_model_create": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(_P)]),

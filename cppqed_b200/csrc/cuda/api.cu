@@ -14,36 +14,14 @@
 #include <string>
 #include <vector>
 
-#include "../host/errors.hpp"
-#include "../host/lowering.hpp"
-#include "cqg.h"
-#include "mcwf_block.cuh"
-#include "mcwf_kernel.cuh"
+#include "engine_internal.cuh"
 
 using cqg::fail;
 using cqg::guarded;
 namespace dev = cqg::dev;
+using namespace cqg::engine;
 
 namespace {
-
-struct CudaError : std::runtime_error {
-  using std::runtime_error::runtime_error;
-};
-
-void ck(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <typename F>
-int guardedCuda(F&& f) {
-  return guarded([&]() -> int {
-    try {
-      return f();
-    } catch (const CudaError& e) {
-      return fail(CQG_E_CUDA, e.what());
-    }
-  });
-}
 
 // single device allocation carved into aligned sub-buffers
 struct Arena {
@@ -57,31 +35,6 @@ struct Arena {
 };
 
 }  // namespace
-
-struct cqg_system {
-  cqg::LoweredSystem L;
-  int device = 0;
-  void* dmem = nullptr;
-  dev::SysDev sd{};
-  ~cqg_system() {
-    if (dmem) cudaFree(dmem);
-  }
-};
-
-// One persistent launch per run call: the trajectories of one kernel shape, a segment of
-// the ensemble's order array, on their own stream.
-struct KernelGroup {
-  int kind = 0;     // 0: warp per trajectory, 1: CTA per trajectory
-  int E = 0;        // warp kind: rows per lane
-  int smax = 0;     // off-diagonal slots per row (max over the group's systems)
-  int Dmax = 0;
-  int threads = 0;  // CTA size
-  int64_t first = 0, count = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t done = nullptr;
-  void* scratch = nullptr;  // block kind: per-CTA stage vectors
-  size_t scratchBytes = 0;
-};
 
 struct cqg_ensemble {
   int device = 0;
@@ -126,12 +79,10 @@ struct cqg_ensemble {
   }
 };
 
-namespace {
+namespace cqg {
+namespace engine {
 
-using dcomp = std::complex<double>;
-
-// rates of the initial state (the MCWF_Trajectory constructor, MCWF_Trajectory.h:114-117)
-std::vector<double> hostRates(const cqg::LoweredSystem& L, const std::vector<dcomp>& psi) {
+std::vector<double> hostRates(const LoweredSystem& L, const std::vector<dcomp>& psi) {
   std::vector<double> r(L.jumps.size());
   for (size_t m = 0; m < L.jumps.size(); ++m) {
     if (!L.weights[m].empty()) {
@@ -151,6 +102,25 @@ std::vector<double> hostRates(const cqg::LoweredSystem& L, const std::vector<dco
   }
   return r;
 }
+
+double initialDtTry(const cqg_system& s, const std::vector<dcomp>& psi, const cqg_mcwf_pars& p, bool* overshot) {
+  double dt0 = p.dt_init > 0 ? p.dt_init : 1. / (10. * s.L.highestFrequency);
+  *overshot = false;
+  // MCWF_Trajectory constructor: dpLimit should not be overshot at startup either
+  if (p.noise && !s.L.jumps.empty()) {
+    double totalRate = 0.;
+    for (double r : hostRates(s.L, psi)) totalRate += r;
+    const double suggested = p.dp_limit / totalRate;
+    *overshot = totalRate * dt0 > p.dp_limit;
+    dt0 = s.L.hasH ? std::min(dt0, suggested) : suggested;
+  }
+  return dt0;
+}
+
+}  // namespace engine
+}  // namespace cqg
+
+namespace {
 
 template <typename T>
 void upload(void* base, size_t off, const std::vector<T>& v) {
@@ -291,12 +261,6 @@ BlockKernelFn pick_block(bool fp64);
 
 namespace {
 
-// the warp kernel holds up to 4 rows per lane
-constexpr int kWarpKernelMaxD = 128;
-// kernel groups: warp kernel with E = 1..4 rows per lane, and the block kernel
-constexpr int kMaxGroups = 5;
-
-int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
 
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
                  const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars);
@@ -397,7 +361,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   std::vector<double> t(nTraj, 0.), t0(nTraj, 0.), dtTry(nTraj), dtDid(nTraj, 0.);
   std::vector<unsigned long long> rng(4 * nTraj, 0), cnt(8 * nTraj, 0);
   std::vector<unsigned char> psiBytes(size_t(psiElems) * e->elemBytes);
-  std::vector<double> initRates;
+  double dt0Shared = 0.;
+  bool overshotShared = false;
   for (int64_t i = 0; i < nTraj; ++i) {
     const cqg_system* s = systems[e->sysIdx[i]];
     const int64_t D = s->L.D;
@@ -413,7 +378,6 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
         std::memcpy(&psiBytes[(e->psiOff[i] + k) * 8], &v, 8);
       }
     }
-    double dt0 = pars->dt_init > 0 ? pars->dt_init : 1. / (10. * s->L.highestFrequency);
     if (pars->rng == CQG_RNG_PCG64) {
       const auto g = dev::Pcg64::seeded(pars->seed, pars->prng_stream + uint64_t(i));
       rng[4 * i + 0] = g.state.hi;
@@ -421,16 +385,10 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       rng[4 * i + 2] = g.inc.hi;
       rng[4 * i + 3] = g.inc.lo;
     }
-    // MCWF_Trajectory constructor: dpLimit should not be overshot at startup either
-    if (pars->noise && !s->L.jumps.empty()) {
-      if (psi0Off || i == 0) initRates = hostRates(s->L, psi);
-      double totalRate = 0.;
-      for (double r : initRates) totalRate += r;
-      const double suggested = pars->dp_limit / totalRate;
-      if (totalRate * dt0 > pars->dp_limit) cnt[8 * i + 4] += 1;
-      dt0 = s->L.hasH ? std::min(dt0, suggested) : suggested;
-    }
-    dtTry[i] = dt0;
+    // one initial state for the whole ensemble: its initial step once
+    if (psi0Off || i == 0) dt0Shared = initialDtTry(*s, psi, *pars, &overshotShared);
+    if (overshotShared) cnt[8 * i + 4] += 1;
+    dtTry[i] = dt0Shared;
   }
   ck(cudaMemcpy(b + oPsi, psiBytes.data(), psiBytes.size(), cudaMemcpyHostToDevice), "cudaMemcpy(psi)");
   upload(b, oOff, e->psiOff);
@@ -512,14 +470,18 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   return CQG_OK;
 }
 
-// One persistent launch of a kernel group on stream st.
-void launchGroup(cqg_ensemble& e, KernelGroup& g, dev::RunArgs ra, int nSM, cudaStream_t st) {
-  const bool fp64 = e.pars.precision == CQG_FP64;
-  dev::TrajDev tdArg = e.td;
+}  // namespace
+
+namespace cqg {
+namespace engine {
+
+void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGroup& g, dev::RunArgs ra, int nSM,
+                 cudaStream_t st) {
+  dev::TrajDev tdArg = td;
   if (g.kind == 0) {
     KernelFn fn = pickKernel(fp64, g.E, g.smax);
     const int warps = g.threads / 32;
-    const size_t smem = size_t(warps) * 3 * 32 * g.E * e.elemBytes + size_t(warps) * sizeof(dev::WarpScratch);
+    const size_t smem = size_t(warps) * 3 * 32 * g.E * elemBytes + size_t(warps) * sizeof(dev::WarpScratch);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -535,7 +497,7 @@ void launchGroup(cqg_ensemble& e, KernelGroup& g, dev::RunArgs ra, int nSM, cuda
     // per-CTA scratch slab
     dev::BlockKernelFn fn = dev::pick_block(fp64);
     int smemD = g.Dmax;
-    const size_t smem = 2 * size_t(smemD) * e.elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+    const size_t smem = 2 * size_t(smemD) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -545,7 +507,7 @@ void launchGroup(cqg_ensemble& e, KernelGroup& g, dev::RunArgs ra, int nSM, cuda
     grid = std::max(grid, 1);
     dev::BlockScratch bsc;
     bsc.stride = (g.Dmax + 31) / 32 * 32;
-    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * e.elemBytes;
+    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * elemBytes;
     if (need > g.scratchBytes) {
       if (g.scratch) {
         ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
@@ -561,6 +523,11 @@ void launchGroup(cqg_ensemble& e, KernelGroup& g, dev::RunArgs ra, int nSM, cuda
        "kernel launch");
   }
 }
+
+}  // namespace engine
+}  // namespace cqg
+
+namespace {
 
 int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   ck(cudaSetDevice(e->device), "cudaSetDevice");
@@ -608,7 +575,7 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
     ra.order = e->dOrder + g.first;
     ra.nTasks = int(g.count);
     ra.queue = e->dQueue + gi;
-    launchGroup(*e, g, ra, nSM, st);
+    launchGroup(e->pars.precision == CQG_FP64, e->elemBytes, e->td, g, ra, nSM, st);
     if (fork) {
       ck(cudaEventRecord(g.done, st), "cudaEventRecord");
       ck(cudaStreamWaitEvent(e->stream, g.done, 0), "cudaStreamWaitEvent");

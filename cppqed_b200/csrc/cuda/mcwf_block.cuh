@@ -415,7 +415,7 @@ struct BlockWorker {
         for (int s = 0; s < ra.nSteps && t < ra.T; ++s)
           if (!step(ra.T - t, td)) break;
       } else {
-        const double endTime = ra.mode == RUN_TO ? ra.tEnd : t + ra.Dt;
+        const double endTime = ra.mode == RUN_TO ? (ra.tEndPer ? ra.tEndPer[ti] : ra.tEnd) : t + ra.Dt;
         double dt;
         while ((dt = endTime - t) != 0.) {
           if (dt < 0. || ++guard > ra.maxStepsPerInterval ||

@@ -192,6 +192,7 @@ struct RunArgs {
   double Dt;        // RUN_INTERVALS
   int nIntervals;   // RUN_INTERVALS / RUN_STEPS
   double tEnd;      // RUN_TO
+  const double* tEndPer;  // RUN_TO: per-trajectory end times (indexed like the trajectory arrays) or null
   int nSteps;       // RUN_STEPS: steps per interval
   double T;         // RUN_STEPS: end time
   double absSlot, relSlot;  // Odeint error-checker slots (eps_abs, eps_rel after the swap)
@@ -693,7 +694,7 @@ struct Worker {
         for (int s = 0; s < ra.nSteps && t < ra.T; ++s)
           if (!step(ra.T - t, td)) break;
       } else {
-        const double endTime = ra.mode == RUN_TO ? ra.tEnd : t + ra.Dt;
+        const double endTime = ra.mode == RUN_TO ? (ra.tEndPer ? ra.tEndPer[ti] : ra.tEnd) : t + ra.Dt;
         double dt;
         while ((dt = endTime - t) != 0.) {
           // bounded: a negative remainder, a step budget, or the wall-clock watchdog

@@ -269,3 +269,69 @@ def probe_fma_peaks():
     b = C.c_double()
     check(lib().cqg_probe_fma_peaks(C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+class Server:
+    """Continuous-batching request server (cqg_server_*)."""
+
+    def __init__(self, pars=None, hbm_budget_bytes=None, max_trajectories=None, max_averages=None):
+        p = A.cqg_server_pars()
+        lib().cqg_server_pars_default(C.byref(p))
+        if pars is not None:
+            p.mcwf = pars
+        if hbm_budget_bytes is not None:
+            p.hbm_budget_bytes = int(hbm_budget_bytes)
+        if max_trajectories is not None:
+            p.max_trajectories = int(max_trajectories)
+        if max_averages is not None:
+            p.max_averages = int(max_averages)
+        h = C.c_void_p()
+        check(lib().cqg_server_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().cqg_server_destroy(self._h)
+            self._h = None
+
+    def submit(self, system, psi0, n_traj, T, Dt, prng_stream):
+        self._keep.append(system)
+        buf, _keep = to_c(psi0)
+        rid = C.c_int64()
+        check(lib().cqg_server_submit(self._h, system._h, buf, int(n_traj), float(T), float(Dt), int(prng_stream),
+                                      C.byref(rid)))
+        return rid.value
+
+    def round(self):
+        a = C.c_int32()
+        w = C.c_int32()
+        check(lib().cqg_server_round(self._h, C.byref(a), C.byref(w)))
+        return a.value, w.value
+
+    def completed(self):
+        n = C.c_int32()
+        check(lib().cqg_server_completed(self._h, None, 0, C.byref(n)))
+        ids = (C.c_int64 * max(n.value, 1))()
+        check(lib().cqg_server_completed(self._h, ids, n.value, C.byref(n)))
+        return list(ids[:n.value])
+
+    def result(self, rid):
+        """(rows [n_rows, n_avr + 1] of ensemble sums, accepted steps, (submit, admit, done) s, status)."""
+        nr = C.c_int32()
+        nc = C.c_int32()
+        check(lib().cqg_server_result(self._h, int(rid), None, 0, C.byref(nr), C.byref(nc), None, None, None))
+        rows = np.zeros((nr.value, nc.value))
+        steps = C.c_uint64()
+        times = (C.c_double * 3)()
+        st = C.c_uint32()
+        check(lib().cqg_server_result(self._h, int(rid), rows.ctypes.data_as(C.POINTER(C.c_double)), nr.value,
+                                      C.byref(nr), C.byref(nc), C.byref(steps), times, C.byref(st)))
+        return rows, steps.value, tuple(times), st.value
+
+    def stats(self):
+        s = C.c_uint64()
+        ms = C.c_double()
+        r = C.c_int64()
+        check(lib().cqg_server_stats(self._h, C.byref(s), C.byref(ms), C.byref(r)))
+        return s.value, ms.value, r.value

@@ -241,6 +241,47 @@ int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, doub
  * kind), off-diagonal slot bound, CTA threads, trajectories in the group. */
 int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap);
 
+/* ---- request server ------------------------------------------------------
+ * Continuous batching of ensemble requests (no reference counterpart: C++QED runs one
+ * ensemble at a time, Ensemble::advance, StochasticTrajectory.h:220-245).  A request is a
+ * system, an initial state, n_traj trajectories (pcg64 streams prng_stream + i, as in an
+ * ensemble), an end time T and an output interval Dt; its result is one row of ensemble
+ * sums per interval (the system's n_avr linear averages, then the dtDid column), exactly the
+ * rows cqg_ensemble_run would give for the same request alone.  Each cqg_server_round
+ * admits waiting requests in arrival order whose trajectories fit the free slots and whose
+ * states fit the free state heap (hbm_budget_bytes), then advances every admitted request
+ * by one output interval in shared launches, and retires those that reached T.  Not thread
+ * safe per server.                                                                     */
+typedef struct cqg_server_pars {
+  uint64_t hbm_budget_bytes;  /* slot tables + state heap on the device */
+  int32_t max_trajectories;   /* slots */
+  int32_t max_systems;        /* distinct systems over the server's life */
+  int32_t max_averages;       /* largest n_avr of a request's system */
+  int32_t reserved;
+  cqg_mcwf_pars mcwf;         /* shared by every request (prng_stream per request) */
+} cqg_server_pars;
+
+typedef struct cqg_server cqg_server;
+void cqg_server_pars_default(cqg_server_pars* p);
+int cqg_server_create(const cqg_server_pars* p, cqg_server** out);
+/* Queues a request; psi0 is copied.  The request id identifies it in the calls below. */
+int cqg_server_submit(cqg_server* s, const cqg_system* sys, const cqg_complex* psi0, int64_t n_traj, double T,
+                      double Dt, uint64_t prng_stream, int64_t* request_id);
+/* One scheduling round (admit, advance one interval, retire); returns after the round's
+ * device work.  n_active / n_waiting (may be NULL): requests on the device / still queued. */
+int cqg_server_round(cqg_server* s, int32_t* n_active, int32_t* n_waiting);
+/* Ids of finished requests not yet collected (all of them in *n; the first cap in ids). */
+int cqg_server_completed(cqg_server* s, int64_t* ids, int32_t cap, int32_t* n);
+/* Result of a finished request: n_rows x n_cols sums (rows may be NULL to query the size),
+ * accepted MCWF steps, times[3] = submit, admission and completion in seconds since the
+ * server's creation, and the OR of its trajectories' status words.  A call with
+ * cap_rows >= n_rows delivers the result and forgets the request. */
+int cqg_server_result(cqg_server* s, int64_t id, double* rows, int32_t cap_rows, int32_t* n_rows, int32_t* n_cols,
+                      uint64_t* steps, double* times, uint32_t* status);
+/* Accepted steps of the finished requests, device time of the rounds' MCWF launches, rounds. */
+int cqg_server_stats(const cqg_server* s, uint64_t* steps, double* kernel_ms, int64_t* rounds);
+int cqg_server_destroy(cqg_server* s);
+
 /* Measured FMA throughput of the current device (TFLOP/s, 2 flops per FMA) for
  * FP64 and FP32 CUDA cores: the denominator of the kernels' roofline and an
  * input of the launch-shape tuner.  Runs two short probe kernels. */
