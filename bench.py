@@ -33,6 +33,11 @@ WORKLOADS = {
     "qbitmode_jc_2x40": ("QbitMode_C++QED",
                          ["--picture", "Sch", "--deltaA", "0", "--gamma", "0.5", "--deltaC", "0", "--kappa", "1",
                           "--eta", "1.5", "--cutoff", "40", "--g", "2"], 4096, 1.0),
+    # particle in a cavity (1particle1mode, ParticleAlongCavity with a cos^2 mode function,
+    # no transverse pump): mode cutoff 20 x particle momenta 2^7 = 2560
+    "particle_cavity_2560": ("1particle1mode",
+                             ["--1p1mconf", "2", "--vClass", "0", "--modeCav", "Cos", "--kCav", "1", "--Unot", "-1",
+                              "--eta", "5", "--kappa", "1", "--cutoff", "20", "--fin", "7"], 2048, 0.05),
     "pumped_lossy_mode_30": ("PumpedLossyMode_C++QED",
                              ["--picture", "Sch", "--deltaC", "-1", "--eta", "2", "--kappa", "1", "--cutoff", "30",
                               "--no_quadratures"], 1000, 1.0),
@@ -240,6 +245,7 @@ def run_apply(model, n_states=1 << 20, warmup=3, reps=20):
 
     system = cqg.System(model.desc)
     D = model.dim
+    n_states = max(1, min(n_states, (4 << 30) // (48 * D)))  # at most ~4 GB moved per launch
     g = torch.Generator(device="cuda").manual_seed(5)
     psi = torch.randn(n_states, D, dtype=torch.complex128, device="cuda", generator=g)
     dpsi = torch.zeros_like(psi)

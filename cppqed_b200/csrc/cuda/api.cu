@@ -150,7 +150,7 @@ void buildSystemDevice(cqg_system& s) {
   std::vector<int> jcol(size_t(nJ) * SJ * D), ocol(size_t(nObs) * SO * D);
   std::vector<dcomp> jval(size_t(nJ) * SJ * D), oval(size_t(nObs) * SO * D);
   std::vector<double> jw(size_t(nJ) * D, 0.);
-  std::vector<int> jHasW(nJ), oRe(nObs), oIm(nObs);
+  std::vector<int> jHasW(nJ), oRe(nObs), oIm(nObs), oS(nObs);
   for (int m = 0; m < nJ; ++m) {
     const auto& J = L.jumps[m];
     for (int k = 0; k < SJ; ++k)
@@ -172,12 +172,13 @@ void buildSystemDevice(cqg_system& s) {
       }
     oRe[q] = L.obsColRe[q];
     oIm[q] = L.obsColIm[q];
+    oS[q] = O.S;
   }
   const auto& H = L.ham;
   const int S = H.S;
   const size_t oCol = A.add(H.col.size() * 4 + 4), oJcol = A.add(jcol.size() * 4 + 4), oJw = A.add(jw.size() * 8 + 8),
                oJHasW = A.add(jHasW.size() * 4 + 4), oOcol = A.add(ocol.size() * 4 + 4),
-               oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4),
+               oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4), oOS = A.add(oS.size() * 4 + 4),
                oFreq = A.add(H.freq.size() * 16 + 16), oLambda = A.add(L.lambda.size() * 16 + 16),
                oDiagD = A.add(H.diag.size() * 16 + 16), oValD = A.add(H.val.size() * 16 + 16),
                oJvalD = A.add(jval.size() * 16 + 16), oDiagF = A.add(H.diag.size() * 8 + 8),
@@ -192,6 +193,7 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oOval, toD2(oval));
   upload(b, oORe, oRe);
   upload(b, oOIm, oIm);
+  upload(b, oOS, oS);
   upload(b, oFreq, toD2(H.freq));
   upload(b, oLambda, toD2(L.lambda));
   upload(b, oDiagD, toD2(H.diag));
@@ -219,6 +221,7 @@ void buildSystemDevice(cqg_system& s) {
   sd.oval = reinterpret_cast<const double2*>(b + oOval);
   sd.oRe = reinterpret_cast<const int*>(b + oORe);
   sd.oIm = reinterpret_cast<const int*>(b + oOIm);
+  sd.oS = reinterpret_cast<const int*>(b + oOS);
   sd.freq = H.freq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFreq);
   sd.lambda = L.lambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oLambda);
   sd.diagD = reinterpret_cast<const double2*>(b + oDiagD);
@@ -324,7 +327,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   }
   if (int64_t(e->Dmax) * 2 * (pars->precision == CQG_FP64 ? 16 : 8) > 200 * 1024)
     return fail(CQG_E_UNSUPPORTED, "ensemble: the stage vectors of a trajectory exceed shared memory");
-  if (e->Smax > 8) return fail(CQG_E_UNSUPPORTED, "ensemble: more than 8 off-diagonal entries per row");
+  if (e->Smax > kMaxSlots) return fail(CQG_E_UNSUPPORTED, "ensemble: more than 64 off-diagonal entries per row");
   e->device = systems[0]->device;
   ck(cudaSetDevice(e->device), "cudaSetDevice");
   ck(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -428,24 +431,24 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   // kernel groups: CTA-per-trajectory for D > 128, else warp-per-trajectory by rows per
   // lane; heavier groups first, and inside a group the longest trajectories first
   // (dimension as the cost proxy) for its work queue
-  auto groupKey = [&](int64_t i) {
-    const int D = int(systems[e->sysIdx[i]]->L.D);
-    return D <= kWarpKernelMaxD ? (D + 31) / 32 : kMaxGroups;
+  auto trajKey = [&](int64_t i) {
+    const cqg_system* sy = systems[e->sysIdx[i]];
+    return groupKey(sy->L.D, sy->sd.S);
   };
   std::vector<int> order(nTraj);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-    const int ka = groupKey(a), kc = groupKey(c);
+    const int ka = trajKey(a), kc = trajKey(c);
     if (ka != kc) return ka > kc;
     return systems[e->sysIdx[a]]->L.D > systems[e->sysIdx[c]]->L.D;
   });
   for (int64_t k = 0; k < nTraj;) {
     KernelGroup g;
-    const int key = groupKey(order[k]);
+    const int key = trajKey(order[k]);
     g.kind = key == kMaxGroups ? 1 : 0;
     g.E = g.kind ? 0 : key;
     g.first = k;
-    for (; k < nTraj && groupKey(order[k]) == key; ++k) {
+    for (; k < nTraj && trajKey(order[k]) == key; ++k) {
       const cqg_system* s = systems[e->sysIdx[order[k]]];
       g.Dmax = std::max<int>(g.Dmax, int(s->L.D));
       g.smax = std::max(g.smax, s->sd.S);

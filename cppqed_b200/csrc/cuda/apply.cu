@@ -14,7 +14,7 @@
 // thread owns fixed rows, so its coefficients (with the interaction-picture phase
 // exp(tau * freq) already applied) sit in registers for the whole launch.
 // Fallback (elementApplyKernel): a grid-stride walk over elements with the gathers from
-// global memory, for more than 4 off-diagonal slots or states too large for the
+// global memory, for more than 4 off-diagonal slots (any number) or states too large for the
 // shared-memory stages.  Both kernels move complex numbers as 16-byte vectors, so the entry
 // point refuses psi / dpsi pointers that are not 16-byte aligned.
 #include <cuda_runtime.h>
@@ -47,8 +47,7 @@ __device__ __forceinline__ double2 applyRow(const SysDev& sys, const double2* __
   acc = cqg::dev::cfma(__ldg(&sys.diagD[r]), __ldg(&x[r]), acc);
   const int nS = S >= 0 ? S : sys.S;
 #pragma unroll
-  for (int s = 0; s < (S >= 0 ? S : 8); ++s) {
-    if (S < 0 && s >= nS) break;
+  for (int s = 0; s < (S >= 0 ? S : nS); ++s) {
     double2 c = __ldg(&sys.valD[s * D + r]);
     if (sys.freq) {
       const double2 f = __ldg(&sys.freq[s * D + r]);
@@ -300,7 +299,6 @@ extern "C" int cqg_system_apply_hamiltonian(const cqg_system* sys, const cqg_com
   if (!sys || !psi || !dpsi || n_states < 1)
     return fail(CQG_E_INVALID, "cqg_system_apply_hamiltonian: null pointer or no states");
   const SysDev* sd = cqg::dev::systemDescriptor(sys);
-  if (sd->S > 8) return fail(CQG_E_UNSUPPORTED, "cqg_system_apply_hamiltonian: more than 8 off-diagonal slots per row");
   int device = 0, nSM = 0;
   cudaError_t err = cudaGetDevice(&device);
   if (err == cudaSuccess) err = cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, device);

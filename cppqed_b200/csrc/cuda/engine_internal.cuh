@@ -55,9 +55,16 @@ constexpr int kWarpKernelMaxD = 128;
 // kernel groups: warp kernel with E = 1..4 rows per lane, and the block kernel
 constexpr int kMaxGroups = 5;
 
-// Group key of a trajectory of dimension D: rows per lane 1..4, or kMaxGroups for the
-// CTA-per-trajectory kernel.
-inline int groupKey(int64_t D) { return D <= kWarpKernelMaxD ? int((D + 31) / 32) : kMaxGroups; }
+// the warp kernel keeps up to 8 off-diagonal slots per row in registers; the CTA kernel
+// walks any number up to kMaxSlots
+constexpr int kWarpKernelMaxS = 8;
+constexpr int kMaxSlots = 64;
+
+// Group key of a trajectory of dimension D with S off-diagonal slots per row: rows per lane
+// 1..4 (warp kernel), or kMaxGroups for the CTA-per-trajectory kernel.
+inline int groupKey(int64_t D, int S) {
+  return D <= kWarpKernelMaxD && S <= kWarpKernelMaxS ? int((D + 31) / 32) : kMaxGroups;
+}
 
 // One persistent launch per run call: the trajectories of one kernel shape, a segment of
 // an order array, on their own stream.

@@ -372,10 +372,11 @@ struct BlockWorker {
     for (int k = 0; k < nObs; ++k) {
       const double2* ov = sysp->oval + size_t(k) * SO * D;
       const int* oc = sysp->ocol + size_t(k) * SO * D;
+      const int nSk = sysp->oS[k];
       double v[2] = {0., 0.};
       for (int r = threadIdx.x; r < D; r += blockDim.x) {
         double2 acc = make_double2(0., 0.);
-        for (int s = 0; s < SO; ++s) {
+        for (int s = 0; s < nSk; ++s) {
           const C2 y = ys0[oc[s * D + r]];
           acc = cfma(ov[s * D + r], make_double2(double(y.x), double(y.y)), acc);
         }

@@ -139,6 +139,7 @@ struct SysDev {
   const double2* oval;   // [nObs][SO][D]
   const int* oRe;        // [nObs]
   const int* oIm;        // [nObs]
+  const int* oS;         // [nObs] slots used by each observable (<= SO; the rest is padding)
   const double2* freq;   // [S][D] (IP) or null
   const double2* lambda; // [D] (Exact) or null
   // precision-specific copies
@@ -644,12 +645,13 @@ struct Worker {
     for (int k = 0; k < nObs; ++k) {
       const double2* ov = sysp->oval + size_t(k) * SO * D;
       const int* oc = sysp->ocol + size_t(k) * SO * D;
+      const int nSk = sysp->oS[k];
       double re = 0., im = 0.;
 #pragma unroll
       for (int e = 0; e < E; ++e)
         if (valid(e)) {
           double2 acc = make_double2(0., 0.);
-          for (int s = 0; s < SO; ++s) {
+          for (int s = 0; s < nSk; ++s) {
             const C2 v = buf0[oc[s * D + row(e)]];
             acc = cfma(ov[s * D + row(e)], make_double2(double(v.x), double(v.y)), acc);
           }

@@ -290,7 +290,7 @@ void advance(cqg_server& s) {
     putAsync(s.dTEnd + r.slot0, tEnd, st);
     segFirst[q] = int(r.slot0);
     segCount[q] = int(r.nTraj);
-    const int key = groupKey(r.sys->L.D);
+    const int key = groupKey(r.sys->L.D, r.sys->sd.S);
     for (int64_t i = 0; i < r.nTraj; ++i) byGroup[key].push_back({r.sys->L.D, int(r.slot0 + i)});
   }
   std::vector<int> order;
@@ -310,7 +310,7 @@ void advance(cqg_server& s) {
       g.Dmax = std::max<int>(g.Dmax, int(p.first));
     }
     for (auto& req : s.active)
-      if (groupKey(req->sys->L.D) == key) g.smax = std::max(g.smax, req->sys->sd.S);
+      if (groupKey(req->sys->L.D, req->sys->sd.S) == key) g.smax = std::max(g.smax, req->sys->sd.S);
     launch.push_back(&g);
   }
   putAsync(s.dOrder, order, st);
@@ -517,7 +517,8 @@ int cqg_server_submit(cqg_server* s, const cqg_system* sys, const cqg_complex* p
     if (sys->L.nAvr + 1 > s->stride) return fail(CQG_E_UNSUPPORTED, "cqg_server_submit: more averages than max_averages");
     if (int(sys->L.jumps.size()) > dev::MAX_JUMPS)
       return fail(CQG_E_UNSUPPORTED, "cqg_server_submit: more than 8 jump operators");
-    if (sys->sd.S > 8) return fail(CQG_E_UNSUPPORTED, "cqg_server_submit: more than 8 off-diagonal entries per row");
+    if (sys->sd.S > kMaxSlots)
+      return fail(CQG_E_UNSUPPORTED, "cqg_server_submit: more than 64 off-diagonal entries per row");
     if (int64_t(sys->L.D) * 2 * int64_t(s->elemBytes) > 200 * 1024)
       return fail(CQG_E_UNSUPPORTED, "cqg_server_submit: the stage vectors of a trajectory exceed shared memory");
     if (n_traj > s->maxTraj || n_traj * sys->L.D > s->maxElems)

@@ -541,4 +541,429 @@ ElementPtr make(const ElementPtr& m0, const ElementPtr& m1, Kind kind, dcomp u) 
 
 }  // namespace coupledmodes
 
+////////////////////////////////////////////////////////////////////////////////
+// Mode functions (ModeFunction.cc), Particle (Particle.cc), ParticleCavity
+// (ParticleCavity.cc), ParticleTwoModes (ParticleTwoModes.cc)
+////////////////////////////////////////////////////////////////////////////////
+
+std::istream& operator>>(std::istream& is, ModeFunctionType& mf) {
+  std::string s;
+  is >> s;
+  if (s == "Sin")
+    mf = ModeFunctionType::Sin;
+  else if (s == "Cos")
+    mf = ModeFunctionType::Cos;
+  else if (s == "Plus")
+    mf = ModeFunctionType::Plus;
+  else if (s == "Minus")
+    mf = ModeFunctionType::Minus;
+  else
+    is.setstate(std::ios_base::failbit);
+  return is;
+}
+
+namespace {
+const double kPi = 3.14159265358979323846;
+int gslSign(double x) { return x >= 0. ? 1 : -1; }  // GSL_SIGN, used by cppqedutils::sign
+}  // namespace
+
+namespace particle {
+
+std::istream& operator>>(std::istream& is, InitialCondition& ic) {
+  std::string s;
+  is >> s;
+  if (s.size() < 2 || s.front() != '(' || s.back() != ')') {
+    is.setstate(std::ios_base::failbit);
+    return is;
+  }
+  std::string body = s.substr(1, s.size() - 2);
+  for (char& c : body)
+    if (c == ',') c = ' ';
+  std::istringstream in(body);
+  InitialCondition r;
+  std::string flag;
+  in >> r.x0 >> r.k0 >> r.sig >> flag;
+  if (in.fail()) {
+    is.setstate(std::ios_base::failbit);
+    return is;
+  }
+  r.inK = flag == "1" || flag == "true";
+  ic = r;
+  return is;
+}
+
+Pars::Pars(ParameterTable& p, const std::string& mod) {
+  omrec = p.add<double>("omrec", mod, 1.);
+  fin = p.add<size_t>("fin", mod, 6);
+  init = p.add<InitialCondition>("pinit", mod, InitialCondition{});
+  hoInitn = p.add<int>("HOinitn", mod, -1);
+}
+
+ParsPumped::ParsPumped(ParameterTable& p, const std::string& mod) : Pars(p, mod) {
+  vClass = p.add<double>("vClass", mod, -10.);
+  kPart = p.add<size_t>("kPart", mod, 1);
+  modePart = p.add<ModeFunctionType>("modePart", mod, ModeFunctionType::Sin);
+}
+
+Spatial::Spatial(size_t f, double dk) : fin(f), deltaK(dk) {
+  xMax = kPi / deltaK;
+  deltaX = 2 * xMax / double(size_t(1) << fin);
+  kMax = kPi / deltaX;
+}
+
+void ffTransform(CVec& psi, Direction dir) {
+  const size_t N = psi.size();
+  if (N < 2) return;
+  const double sgn = dir == Direction::XK ? -1. : 1.;
+  CVec y(N);
+  for (size_t k = 0; k < N; ++k) {
+    dcomp acc = 0;
+    for (size_t j = 0; j < N; ++j) {
+      const double ang = sgn * 2. * kPi * double((j * k) % N) / double(N);
+      acc += psi[j] * dcomp(std::cos(ang), std::sin(ang));
+    }
+    y[k] = acc;
+  }
+  const double norm = 1. / std::sqrt(double(N));
+  const size_t half = N >> 1;
+  for (size_t m = 0; m < N; ++m) psi[m] = norm * y[(m + half) % N] * ((m & 1) ? -1. : 1.);
+}
+
+namespace {
+
+CVec kSquared(const Spatial& space, dcomp factor) {  // mainDiagonal(space, omrec) (Particle.cc:92-95)
+  CVec d(space.dim());
+  for (size_t i = 0; i < d.size(); ++i) d[i] = factor * space.k(i) * space.k(i);
+  return d;
+}
+
+Tridiagonal expINKXdim(size_t dim, long nK) {  // Particle.cc:60-73
+  const long D = long(dim) - (nK > 0 ? nK : -nK);
+  if (D < 0) return Tridiagonal();
+  CVec ones(size_t(D), dcomp(1., 0.));
+  if (nK > 0) return Tridiagonal::unary({}, size_t(nK), ones, {});
+  if (nK == 0) return Tridiagonal::unary(ones);
+  return Tridiagonal::unary({}, size_t(-nK), {}, ones);
+}
+
+Tridiagonal cosNKXdim(size_t dim, long nK) { return (expINKXdim(dim, nK) + expINKXdim(dim, -nK)) / 2.; }
+
+// the particle's own pump term, H/i (Particle.cc:83-87)
+Tridiagonal pumpHOverI(size_t dim, double vClass, const ModeFunction& mf) {
+  if (vClass && !isComplex(mf.type))
+    return vClass * (mf.type == ModeFunctionType::Sin ? -1. : 1.) * cosNKXdim(dim, mf.k << 1) / (2. * I1);
+  return Tridiagonal();
+}
+
+// particle::Averaged (Particle.cc:128-163): <P>, VAR(P), <X>, DEV(X); <X> and <X^2> are the
+// position-space moments of the k-space state, i.e. of M rho M^+ with M the k -> x transform
+void fillParticleAveraged(Element& e, const Spatial& space) {
+  const size_t N = space.dim();
+  e.avLabels = {"<P>", "VAR(P)", "<X>", "DEV(X)"};
+  CVec dk(N), dk2(N);
+  for (size_t i = 0; i < N; ++i) {
+    dk[i] = space.k(i);
+    dk2[i] = space.k(i) * space.k(i);
+  }
+  std::vector<CVec> M(N, CVec(N));  // M[m][j]: column j = transform of the unit vector e_j
+  for (size_t j = 0; j < N; ++j) {
+    CVec v(N, 0.);
+    v[j] = 1.;
+    ffTransform(v, Direction::KX);
+    for (size_t m = 0; m < N; ++m) M[m][j] = v[m];
+  }
+  auto dense = [&](int power) {
+    CVec O(N * N, 0.);
+    for (size_t i = 0; i < N; ++i)
+      for (size_t j = 0; j < N; ++j) {
+        dcomp acc = 0;
+        for (size_t m = 0; m < N; ++m) acc += std::conj(M[m][i]) * std::pow(space.x(m), power) * M[m][j];
+        O[i * N + j] = acc;
+      }
+    return O;
+  };
+  ElementObservable p, p2, x, x2;
+  p.op = Tridiagonal::unary(dk);
+  p.colRe = 0;
+  p2.op = Tridiagonal::unary(dk2);
+  p2.colRe = 1;
+  x.dense = dense(1);
+  x.colRe = 2;
+  x2.dense = dense(2);
+  x2.colRe = 3;
+  e.obs = {p, p2, x, x2};
+  e.process = [](double* avr) {
+    avr[1] -= avr[0] * avr[0];
+    avr[3] = std::sqrt(avr[3] - avr[2] * avr[2]);
+  };
+}
+
+std::shared_ptr<Element> particleBase(size_t fin) {
+  auto e = std::make_shared<Element>();
+  e->keyTitle = "Particle";
+  e->dims = {size_t(1) << fin};
+  e->fin = fin;
+  fillParticleAveraged(*e, Spatial(fin));
+  return e;
+}
+
+void particleExact(Element& e, const Spatial& space, double omrec) {  // particle::Exact (Particle.cc:33-46)
+  e.particleExact = true;
+  e.omrec = omrec;
+  e.exact = {kSquared(space, dcomp(0., -omrec))};  // U = exp(-i omrec k^2 t)
+}
+
+}  // namespace
+
+// particle::make (Particle.cc:452-456): ParticleSch in the Schroedinger picture, else the
+// free Particle with its Exact part only
+ElementPtr make(const Pars& p, Picture qmp) {
+  const Spatial space(p.fin);
+  auto e = particleBase(p.fin);
+  e->omrec = p.omrec;
+  const double dim = double(space.dim());
+  if (qmp == Picture::Sch) {
+    e->isHamiltonian = true;
+    e->hOverI.push_back(Tridiagonal::unary(kSquared(space, dcomp(0., -p.omrec))));
+    e->highestFrequency = highestFrequencyOf({{p.omrec, dim * dim}}, {});
+  } else {
+    particleExact(*e, space, p.omrec);
+    e->highestFrequency = highestFrequencyOf({{p.omrec, dim}}, {});
+  }
+  return e;
+}
+
+// particle::makePumped (Particle.cc:459-462): PumpedParticleSch / PumpedParticle
+ElementPtr makePumped(const ParsPumped& p, Picture qmp) {
+  const Spatial space(p.fin);
+  auto e = particleBase(p.fin);
+  e->omrec = p.omrec;
+  e->pumpedParticle = true;
+  e->vClass = p.vClass;
+  e->pumpMF = ModeFunction{p.modePart, long(p.kPart)};
+  const double dim = double(space.dim());
+  e->isHamiltonian = true;
+  Tridiagonal pump = pumpHOverI(space.dim(), p.vClass, e->pumpMF);
+  if (qmp == Picture::Sch) {  // Hamiltonian<false>: -i omrec k^2 + pump
+    e->hOverI.push_back(Tridiagonal::unary(kSquared(space, dcomp(0., -p.omrec))) + pump);
+    e->highestFrequency = highestFrequencyOf({{p.omrec, dim * dim}, {p.vClass, 1.}}, {});
+  } else {  // Hamiltonian<true>: the pump term furnished with i omrec k^2, and Exact
+    if (!pump.empty()) e->hOverI.push_back(pump.furnishWithFreqs(kSquared(space, dcomp(0., p.omrec))));
+    particleExact(*e, space, p.omrec);
+    e->highestFrequency = highestFrequencyOf({{p.omrec, dim}, {p.vClass, 1.}}, {});
+  }
+  return e;
+}
+
+CVec wavePacket(const InitialCondition& init, const Spatial& space, bool kFlag) {  // Particle.cc:351-371
+  double offset1 = kPi * init.x0, offset2 = init.k0;
+  if (init.inK) {
+    std::swap(offset1, offset2);
+    offset2 = -offset2;
+  }
+  const size_t N = space.dim();
+  CVec psi(N);
+  for (size_t i = 0; i < N; ++i) {
+    const double a = init.inK ? space.k(i) : space.x(i);
+    psi[i] = std::exp(dcomp(-(a - offset1) * (a - offset1) / (4 * init.sig * init.sig), a * offset2));
+  }
+  if (kFlag && !init.inK)
+    ffTransform(psi, Direction::XK);
+  else if (!kFlag && init.inK)
+    ffTransform(psi, Direction::KX);
+  double n2 = 0;
+  for (auto& c : psi) n2 += std::norm(c);
+  for (auto& c : psi) c /= std::sqrt(n2);
+  return psi;
+}
+
+CVec hoState(int n, const InitialCondition& init, const Spatial& space, bool kFlag) {  // Particle.cc:398-418
+  if (n < 0) n = 0;
+  const double kx0 = kPi * init.x0;
+  const size_t N = space.dim();
+  CVec psi(N);
+  for (size_t j = 0; j < N; ++j) {
+    const double t = (space.x(j) - kx0) / init.sig;
+    double h0 = 1., h1 = 2. * t, h = n == 0 ? h0 : h1;  // physicists' Hermite polynomial H_n(t)
+    for (int m = 1; m < n; ++m) {
+      h = 2. * t * h1 - 2. * double(m) * h0;
+      h0 = h1;
+      h1 = h;
+    }
+    psi[j] = std::exp(-t * t / 2.) * h;
+  }
+  if (kFlag) ffTransform(psi, Direction::XK);
+  double n2 = 0;
+  for (auto& c : psi) n2 += std::norm(c);
+  for (auto& c : psi) c /= std::sqrt(n2);
+  return psi;
+}
+
+CVec init(const Pars& p) {  // Particle.cc:434-441
+  const Spatial space(p.fin);
+  return p.hoInitn < 0 ? wavePacket(p.init, space) : hoState(p.hoInitn, p.init, space);
+}
+
+CVec init(const ParsPumped& p) {
+  // without an initial spread, the ground state of the pump's harmonic approximation
+  // (coherent(ParsPumped), Particle.cc:377-380)
+  const Spatial space(p.fin);
+  InitialCondition ic = p.init;
+  if (!p.init.sig) ic = InitialCondition{p.init.x0, p.init.k0, std::pow(p.omrec / std::fabs(p.vClass), .25) / std::sqrt(2.), false};
+  return p.hoInitn < 0 ? wavePacket(ic, space) : hoState(p.hoInitn, ic, space);
+}
+
+Tridiagonal expINKX(const ElementPtr& particle, long nK) {  // Particle.cc:206-213
+  Tridiagonal res = expINKXdim(particle->dims.at(0), nK);
+  if (particle->particleExact && !res.empty())
+    res.furnishWithFreqs(kSquared(Spatial(particle->fin), dcomp(0., particle->omrec)));
+  return res;
+}
+
+Tridiagonal cosNKX(const ElementPtr& particle, long nK) { return (expINKX(particle, nK) + expINKX(particle, -nK)) / 2.; }
+Tridiagonal sinNKX(const ElementPtr& particle, long nK) {
+  return (expINKX(particle, nK) - expINKX(particle, -nK)) / (2. * I1);
+}
+
+Tridiagonal mfNKX(const ElementPtr& particle, const ModeFunction& mf) {  // Particle.cc:216-227
+  switch (mf.type) {
+    case ModeFunctionType::Sin:
+      return sinNKX(particle, mf.k);
+    case ModeFunctionType::Cos:
+      return cosNKX(particle, mf.k);
+    case ModeFunctionType::Plus:
+      return expINKX(particle, mf.k);
+    case ModeFunctionType::Minus:
+      break;
+  }
+  return expINKX(particle, -mf.k);
+}
+
+Tridiagonal mfComposition(const ElementPtr& particle, const ModeFunction& f1, const ModeFunction& f2) {
+  // Particle.cc:229-336: f1^*(k1 x) f2(k2 x) for |k1| == |k2|
+  using MF = ModeFunctionType;
+  MF mf1 = f1.type, mf2 = f2.type;
+  long nK1 = f1.k, nK2 = f2.k;
+  const long nK = std::labs(nK1);
+  const double sign1 = mf1 == MF::Sin && nK1 < 0 ? -1 : 1;
+  const double sign2 = mf2 == MF::Sin && nK2 < 0 ? -1 : 1;
+  const double sign = sign1 * sign2;
+  if (std::labs(nK1) != std::labs(nK2)) throw std::runtime_error("Not a Tridiagonal");
+  if (mf1 == MF::Plus && nK1 < 0) { mf1 = MF::Minus; nK1 *= -1; }
+  if (mf1 == MF::Minus && nK1 < 0) { mf1 = MF::Plus; nK1 *= -1; }
+  if (mf2 == MF::Plus && nK2 < 0) { mf2 = MF::Minus; nK2 *= -1; }
+  if (mf2 == MF::Minus && nK2 < 0) { mf2 = MF::Plus; nK2 *= -1; }
+  const Tridiagonal id = Tridiagonal::identity(particle->dims.at(0));
+  auto is = [&](MF a, MF b) { return mf1 == a && mf2 == b; };
+  if (is(MF::Sin, MF::Sin)) return sign * (id - cosNKX(particle, 2 * nK)) / 2.;
+  if (is(MF::Cos, MF::Cos)) return (id + cosNKX(particle, 2 * nK)) / 2.;
+  if (is(MF::Sin, MF::Cos) || is(MF::Cos, MF::Sin)) return sign * sinNKX(particle, 2 * nK) / 2.;
+  if (is(MF::Plus, MF::Plus) || is(MF::Minus, MF::Minus)) return id;
+  if (is(MF::Plus, MF::Minus)) return expINKX(particle, -2 * nK);
+  if (is(MF::Minus, MF::Plus)) return expINKX(particle, 2 * nK);
+  if (is(MF::Plus, MF::Sin) || is(MF::Sin, MF::Minus)) return sign * (expINKX(particle, -2 * nK) - id) * I1 / 2.;
+  if (is(MF::Plus, MF::Cos) || is(MF::Cos, MF::Minus)) return (id + expINKX(particle, -2 * nK)) / 2.;
+  if (is(MF::Minus, MF::Cos) || is(MF::Cos, MF::Plus)) return (id + expINKX(particle, 2 * nK)) / 2.;
+  if (!(is(MF::Minus, MF::Sin) || is(MF::Sin, MF::Plus))) throw std::logic_error("In mfComposition");
+  return -sign * (expINKX(particle, 2 * nK) - id) * I1 / 2.;
+}
+
+}  // namespace particle
+
+namespace particlecavity {
+
+namespace {
+
+double etaEff(double uNot, double vClass) {  // ParticleCavity.cc:16-20
+  if (uNot * vClass >= 0) return gslSign(uNot) * std::sqrt(uNot * vClass);
+  throw std::domain_error("Unot VClass sign discrepancy");
+}
+
+Tridiagonal plusHCOverI(const Tridiagonal& t) { return tridiagPlusHC(t) / I1; }  // Tridiagonal.h:347
+
+void dispersive(std::vector<Tridiagonal>& res, const ElementPtr& mode, const ElementPtr& part, double uNot,
+                const ModeFunction& mf) {  // ParticleCavity.cc:23-30
+  if (uNot && !isComplex(mf.type))
+    res.push_back(uNot * mode::nop(mode) * (mf.type == ModeFunctionType::Sin ? -1. : 1.) *
+                  particle::cosNKX(part, mf.k << 1) / (2. * I1));
+}
+
+Tridiagonal interfericOneModeFN(const ElementPtr& mode, const ElementPtr& part, double etaeff, const ModeFunction& mf) {
+  return etaeff * plusHCOverI(mode::aop(mode) * particle::mfNKX(part, mf));
+}
+
+Tridiagonal interfericTwoModeFN(const ElementPtr& mode, const ElementPtr& part, double etaeff, const ModeFunction& mfCav,
+                                const ModeFunction& mfPart) {
+  return etaeff * plusHCOverI(mode::aop(mode).dagger() * particle::mfComposition(part, mfCav, mfPart));
+}
+
+std::shared_ptr<Element> base(const ElementPtr& mode, const ElementPtr& part, double uNot, double etaeff) {
+  auto e = std::make_shared<Element>();  // particlecavity::Base (ParticleCavity.cc:61-66)
+  e->keyTitle = "ParticleCavity";
+  e->dims = {mode->dims.at(0), part->dims.at(0)};
+  e->frees = {mode, part};
+  e->isHamiltonian = true;
+  const double md = double(mode->dims[0]);
+  e->highestFrequency = highestFrequencyOf({{uNot, md}, {etaeff, std::sqrt(md)}}, {});
+  return e;
+}
+
+}  // namespace
+
+ElementPtr orthogonal(const ElementPtr& mode, const ElementPtr& part, double uNot) {  // ParticleCavity.cc:69-80
+  if (!part->pumpedParticle) throw std::invalid_argument("ParticleOrthogonalToCavity needs a pumped particle");
+  const double etaeff = etaEff(uNot, part->vClass);
+  auto e = base(mode, part, uNot, etaeff);
+  e->hOverI.push_back(interfericOneModeFN(mode, part, etaeff, part->pumpMF));
+  return e;
+}
+
+ElementPtr along(const ElementPtr& mode, const ElementPtr& part, double uNot, size_t kCav, ModeFunctionType modeCav,
+                 double vClass) {  // ParticleCavity.cc:83-96 (fillT, :40-45)
+  const double etaeff = etaEff(uNot, vClass);
+  auto e = base(mode, part, uNot, etaeff);
+  const ModeFunction mf{modeCav, long(kCav)};
+  dispersive(e->hOverI, mode, part, uNot, mf);
+  if (etaeff) e->hOverI.push_back(interfericOneModeFN(mode, part, etaeff, mf));
+  return e;
+}
+
+ElementPtr alongPumped(const ElementPtr& mode, const ElementPtr& part, double uNot, size_t kCav,
+                       ModeFunctionType modeCav) {  // ParticleCavity.cc:99-109 (fillTTwoModeFN, :48-55)
+  if (!part->pumpedParticle) throw std::invalid_argument("ParticleAlongCavity: pumped particle expected");
+  const double etaeff = etaEff(uNot, part->vClass);
+  if (long(kCav) != std::labs(part->pumpMF.k))
+    throw std::invalid_argument("ParticleAlongCavity with kCav != |kPart| is not a single Tridiagonal: not supported");
+  auto e = base(mode, part, uNot, etaeff);
+  const ModeFunction mf{modeCav, long(kCav)};
+  dispersive(e->hOverI, mode, part, uNot, mf);
+  if (etaeff) e->hOverI.push_back(interfericTwoModeFN(mode, part, etaeff, mf, part->pumpMF));
+  return e;
+}
+
+}  // namespace particlecavity
+
+namespace particletwomodes {
+
+ElementPtr make(const ElementPtr& m0, const ElementPtr& m1, const ElementPtr& part, double uNot0, double uNot1,
+                const ModeFunction& mf0, const ModeFunction& mf1, double phi) {
+  if (uNot0 * uNot1 < 0) throw std::domain_error("Unots sign discrepancy");
+  if (std::labs(mf0.k) != std::labs(mf1.k))
+    throw std::invalid_argument("ParticleTwoModes with |k0| != |k1| is not a single Tridiagonal: not supported");
+  const dcomp factor = double(gslSign(uNot0)) * std::sqrt(uNot0 * uNot1) * std::exp(I1 * phi);
+  auto e = std::make_shared<Element>();
+  e->keyTitle = "ParticleTwoModes";
+  e->dims = {m0->dims.at(0), m1->dims.at(0), part->dims.at(0)};
+  e->frees = {m0, m1, part};
+  e->isHamiltonian = true;
+  e->hOverI.push_back(tridiagPlusHC((factor * mode::aop(m0).dagger()) * mode::aop(m1) *
+                                    particle::mfComposition(part, mf0, mf1)) /
+                      I1);
+  e->highestFrequency =
+      highestFrequencyOf({{uNot0, std::sqrt(double(m0->dims[0]))}, {uNot1, std::sqrt(double(m1->dims[0]))}}, {});
+  return e;
+}
+
+}  // namespace particletwomodes
+
 }  // namespace cqg

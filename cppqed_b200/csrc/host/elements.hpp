@@ -19,6 +19,14 @@ namespace cqg {
 enum class Picture { IP, UIP, Sch };  // QM_Picture (high/QM_Picture.h), default IP
 Picture parsePicture(const std::string& s);
 
+enum class ModeFunctionType { Sin, Cos, Plus, Minus };  // ModeFunction.h
+std::istream& operator>>(std::istream& is, ModeFunctionType& mf);
+inline bool isComplex(ModeFunctionType mf) { return mf == ModeFunctionType::Plus || mf == ModeFunctionType::Minus; }
+struct ModeFunction {
+  ModeFunctionType type = ModeFunctionType::Sin;
+  long k = 1;
+};
+
 struct ElementJump {
   Tridiagonal J;     // on the element's local axes
   int rateAxis = 0;  // local axis of the closed-form weights
@@ -69,6 +77,10 @@ struct Element {
   bool particleExact = false;
   double omrec = 0;
   size_t fin = 0;
+  // PumpedParticleBase (Particle_.h:199-214): pump strength and mode function
+  bool pumpedParticle = false;
+  double vClass = 0;
+  ModeFunction pumpMF;
 };
 
 // ---- helpers shared by elements ------------------------------------------
@@ -124,5 +136,79 @@ enum class Kind { NX, XX, XX_RWA };  // coupledmodes::Coupling (CoupledModes.h)
 ElementPtr make(const ElementPtr& m0, const ElementPtr& m1, Kind kind, dcomp u);
 }
 
+// ---- Particle (Particle.{h,cc}, Particle_.h, ParsParticle.cc) ---------------------
+
+namespace particle {
+struct InitialCondition {  // ParticleInitialCondition.h: (x0, k0, sig, isInK)
+  double x0 = -.5, k0 = 0, sig = .1;
+  bool inK = false;
+};
+std::istream& operator>>(std::istream& is, InitialCondition& ic);  // "(x0,k0,sig,isInK)"
+
+struct Pars {  // ParsParticle.cc:8-14
+  double omrec = 1;
+  size_t fin = 6;
+  InitialCondition init;
+  int hoInitn = -1;
+  Pars() = default;
+  Pars(ParameterTable& p, const std::string& mod = "");
+};
+struct ParsPumped : Pars {  // ParsParticle.cc:17-23
+  double vClass = -10;
+  size_t kPart = 1;
+  ModeFunctionType modePart = ModeFunctionType::Sin;
+  ParsPumped() = default;
+  ParsPumped(ParameterTable& p, const std::string& mod = "");
+};
+
+// Spatial (Particle.cc:257-272): x_i = deltaX i - xMax, k_i = deltaK i - kMax
+struct Spatial {
+  size_t fin;
+  double xMax, deltaX, kMax, deltaK;
+  explicit Spatial(size_t fin, double deltaK = 1);
+  size_t dim() const { return size_t(1) << fin; }
+  double x(size_t i) const { return deltaX * double(i) - xMax; }
+  double k(size_t i) const { return deltaK * double(i) - kMax; }
+};
+
+enum class Direction { XK, KX };  // fft::Direction: forward (x -> k), backward
+// quantumdata::ffTransform of a vector (LazyDensityOperatorFFT.cc:12-31): radix-2 DFT
+// (sign -1 for XK, +1 for KX, unnormalised), halves swapped with factor N^-1/2, odd
+// entries negated.
+void ffTransform(CVec& psi, Direction dir);
+
+ElementPtr make(const Pars& p, Picture qmp);              // Particle / ParticleSch
+ElementPtr makePumped(const ParsPumped& p, Picture qmp);  // PumpedParticle / PumpedParticleSch
+CVec wavePacket(const InitialCondition& init, const Spatial& space, bool kFlag = true);
+CVec hoState(int n, const InitialCondition& init, const Spatial& space, bool kFlag = true);
+CVec init(const Pars& p);
+CVec init(const ParsPumped& p);
+
+// operators on a particle element, furnished with frequencies in the interaction picture
+Tridiagonal expINKX(const ElementPtr& particle, long nK);
+Tridiagonal cosNKX(const ElementPtr& particle, long nK);
+Tridiagonal sinNKX(const ElementPtr& particle, long nK);
+Tridiagonal mfNKX(const ElementPtr& particle, const ModeFunction& mf);
+Tridiagonal mfComposition(const ElementPtr& particle, const ModeFunction& mf1, const ModeFunction& mf2);
+}  // namespace particle
+
+// ---- ParticleCavity (ParticleCavity.cc), ParticleTwoModes (ParticleTwoModes.cc) ----------
+namespace particlecavity {
+// ParticleOrthogonalToCavity(mode, pumpedParticle, Unot)
+ElementPtr orthogonal(const ElementPtr& mode, const ElementPtr& pumpedParticle, double uNot);
+// ParticleAlongCavity with a particle that is not pumped along the cavity (etaeff from
+// Unot and vClass, 0 for none)
+ElementPtr along(const ElementPtr& mode, const ElementPtr& particle, double uNot, size_t kCav, ModeFunctionType modeCav,
+                 double vClass);
+// ParticleAlongCavity with a pumped particle (the two-mode-function Hamiltonian; only the
+// case kCav == |kPart|, a single Tridiagonal, is supported)
+ElementPtr alongPumped(const ElementPtr& mode, const ElementPtr& pumpedParticle, double uNot, size_t kCav,
+                       ModeFunctionType modeCav);
+}  // namespace particlecavity
+namespace particletwomodes {
+// ParticleTwoModes (ParticleTwoModes.cc:17-33); only |k0| == |k1| (a single Tridiagonal)
+ElementPtr make(const ElementPtr& mode0, const ElementPtr& mode1, const ElementPtr& particle, double uNot0,
+                double uNot1, const ModeFunction& mf0, const ModeFunction& mf1, double phi = 0);
+}
 
 }  // namespace cqg

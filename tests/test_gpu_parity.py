@@ -20,8 +20,12 @@ C1_ARGS = ["--picture", "Sch", "--deltaC", "-1", "--eta", "2", "--kappa", "1", "
 
 
 @pytest.mark.parametrize("run", ["run_PTLA_CPPQED_%s_%s" % (m, e) for m in ("dc", "dt", "ndt")
-                                 for e in ("single", "ensemble")])
-def test_ptla_golden_on_device(gpu, golden, run):
+                                 for e in ("single", "ensemble")] +
+                         ["run_1particle1mode_%s_%s" % (m, e)
+                          for m in ("dc", "dt", "ndt", "ndt_conf2", "ndt_conf3", "ndt_conf4")
+                          for e in ("single", "ensemble")] +
+                         ["run_Ring_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble")])
+def test_golden_on_device(gpu, golden, run):
     g = golden[run]
     rows, ens, model = gpu.evolve(g["script"], g["args"])
     ref = np.array(g["rows"])
@@ -401,3 +405,49 @@ def test_block_kernel_cta_shapes_agree(gpu):
                 agree += 1
                 assert np.linalg.norm(a - b) < 1e-9
         assert agree >= n - 1
+
+
+# ---- particle in a cavity on the CTA-per-trajectory kernel ----
+
+PARTICLE_ARGS = ["--1p1mconf", "2", "--vClass", "0", "--modeCav", "Cos", "--kCav", "1", "--Unot", "-1",
+                 "--eta", "5", "--kappa", "1", "--cutoff", "8", "--fin", "5"]
+
+
+def test_particle_cavity_trajectories_replay_oracle(gpu, oracle):
+    """Mode 8 x particle 32 (D = 256, interaction picture, dense position observables):
+    trajectories with jumps replay the oracle's jump records and states."""
+    model = gpu.Model("1particle1mode", PARTICLE_ARGS)
+    assert model.dim == 256
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    n = 4
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ens.run(0.1, 2)
+    agree = 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.1, 2)
+        jt, jl = ens.jumps(i, 4096)
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
+    assert agree >= n - 1
+
+
+def test_particle_cavity_fp32_averages_track_fp64(gpu):
+    """FP32 states with FP64 control against FP64 on the same streams: batch means of
+    <n>, <P>, <X> within 3 standard errors."""
+    model = gpu.Model("1particle1mode", PARTICLE_ARGS)
+    sysd = gpu.System(model.desc)
+    n = 512
+    out = {}
+    for prec in (A.FP64, A.FP32):
+        pars = model.run_pars().mcwf
+        pars.precision = prec
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        ens.run(0.1, 2)
+        out[prec] = ens.traj_averages()[:, :model.n_avr]
+    a64, a32 = out[A.FP64], out[A.FP32]
+    se = a64.std(axis=0, ddof=1) / np.sqrt(n) + 1e-12
+    z = np.abs(a32.mean(axis=0) - a64.mean(axis=0)) / se
+    assert z.max() < 3, z

@@ -8,10 +8,16 @@ import pytest
 from cppqed_b200 import _abi as A
 
 PTLA = ["run_PTLA_CPPQED_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
+# particle in a cavity (binary mode x particle, interaction picture, configurations 1-4 of
+# ParticleOrthogonalToCavity / ParticleAlongCavity) and the ring cavity (composite
+# particle x mode x mode with ParticleTwoModes)
+PARTICLE = ["run_1particle1mode_%s_%s" % (m, e) for m in ("dc", "dt", "ndt", "ndt_conf2", "ndt_conf3", "ndt_conf4")
+            for e in ("single", "ensemble", "master")]
+RING = ["run_Ring_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
 
 
-@pytest.mark.parametrize("run", PTLA)
-def test_ptla_golden(engine, oracle, golden, run):
+@pytest.mark.parametrize("run", PTLA + PARTICLE + RING)
+def test_golden(engine, oracle, golden, run):
     g = golden[run]
     model = engine.Model(g["script"], g["args"])
     rows = oracle.run(model)
