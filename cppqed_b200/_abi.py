@@ -145,11 +145,13 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_set_state": (C.c_int, [_P, C.c_int64, _CP]),
     "cqg_ensemble_get_times": (C.c_int, [_P, _DP, _DP, _DP]),
     "cqg_ensemble_get_counters": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
-    "cqg_ensemble_get_logger_maxima": (C.c_int, [_P, _DP, _DP]),
+    "cqg_ensemble_get_logger_maxima": (C.c_int, [_P, _DP, _DP, _DP]),
     "cqg_ensemble_get_jumps": (C.c_int, [_P, C.c_int64, C.c_int32, _DP, C.POINTER(C.c_int32),
                                          C.POINTER(C.c_int32)]),
     "cqg_ensemble_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
+    "cqg_ensemble_save": (C.c_int, [_P, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "cqg_ensemble_load": (C.c_int, [_P, C.c_void_p, C.c_uint64]),
     "cqg_ensemble_plan": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
     "cqg_server_pars_default": (None, [C.POINTER(cqg_server_pars)]),

@@ -836,6 +836,101 @@ int cqg_ensemble_traj_averages(cqg_ensemble* ens, double* out) {
   });
 }
 
+namespace {
+
+constexpr char kCheckpointMagic[8] = {'C', 'Q', 'G', 'C', 'K', 'P', 'T', '1'};
+
+struct CheckpointHeader {
+  char magic[8];
+  uint32_t elemBytes, jumpCap;
+  int64_t nTraj, psiElems;
+  uint64_t layoutHash;  // dimensions and system index of every trajectory
+};
+
+// the device arrays of a checkpoint, in order: (pointer, bytes)
+std::vector<std::pair<void*, size_t>> checkpointParts(const cqg_ensemble& e, int64_t psiElems) {
+  const size_t n = size_t(e.nTraj);
+  const auto& td = e.td;
+  return {{td.psi, size_t(psiElems) * e.elemBytes},
+          {td.t, n * 8},
+          {td.t0, n * 8},
+          {td.dtTry, n * 8},
+          {td.dtDid, n * 8},
+          {td.rng, n * 32},
+          {td.cnt, n * 64},
+          {td.maxima, n * 24},
+          {td.status, n * 4},
+          {td.jumpT, n * size_t(td.jumpCap) * 8},
+          {td.jumpL, n * size_t(td.jumpCap) * 4},
+          {td.jumpN, n * 8}};
+}
+
+CheckpointHeader checkpointHeader(const cqg_ensemble& e) {
+  CheckpointHeader h{};
+  std::memcpy(h.magic, kCheckpointMagic, 8);
+  h.elemBytes = uint32_t(e.elemBytes);
+  h.jumpCap = uint32_t(e.td.jumpCap);
+  h.nTraj = e.nTraj;
+  uint64_t hash = 1469598103934665603ull, elems = 0;  // FNV-1a over (D, system index)
+  for (int64_t i = 0; i < e.nTraj; ++i) {
+    const uint64_t D = uint64_t(e.systems[e.sysIdx[i]]->L.D), words[2] = {D, uint64_t(e.sysIdx[i])};
+    for (uint64_t w : words)
+      for (int b = 0; b < 8; ++b) hash = (hash ^ ((w >> (8 * b)) & 0xff)) * 1099511628211ull;
+    elems += D;
+  }
+  h.psiElems = int64_t(elems);
+  h.layoutHash = hash;
+  return h;
+}
+
+}  // namespace
+
+int cqg_ensemble_save(const cqg_ensemble* ens, void* buf, uint64_t cap, uint64_t* size) {
+  return guardedCuda([&] {
+    if (!ens || !size) return fail(CQG_E_INVALID, "cqg_ensemble_save: null argument");
+    const CheckpointHeader h = checkpointHeader(*ens);
+    const auto parts = checkpointParts(*ens, h.psiElems);
+    uint64_t total = sizeof(h);
+    for (auto& p : parts) total += p.second;
+    *size = total;
+    if (!buf || cap < total) return CQG_OK;
+    ck(cudaStreamSynchronize(ens->stream), "cudaStreamSynchronize");
+    char* out = static_cast<char*>(buf);
+    std::memcpy(out, &h, sizeof(h));
+    out += sizeof(h);
+    for (auto& p : parts) {
+      ck(cudaMemcpy(out, p.first, p.second, cudaMemcpyDeviceToHost), "cudaMemcpy(checkpoint)");
+      out += p.second;
+    }
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_load(cqg_ensemble* ens, const void* buf, uint64_t size) {
+  return guardedCuda([&] {
+    if (!ens || !buf) return fail(CQG_E_INVALID, "cqg_ensemble_load: null argument");
+    if (size < sizeof(CheckpointHeader)) return fail(CQG_E_INVALID, "cqg_ensemble_load: truncated checkpoint");
+    CheckpointHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    const CheckpointHeader mine = checkpointHeader(*ens);
+    if (std::memcmp(h.magic, kCheckpointMagic, 8) != 0) return fail(CQG_E_INVALID, "cqg_ensemble_load: not a checkpoint");
+    if (h.elemBytes != mine.elemBytes || h.jumpCap != mine.jumpCap || h.nTraj != mine.nTraj ||
+        h.psiElems != mine.psiElems || h.layoutHash != mine.layoutHash)
+      return fail(CQG_E_INVALID, "cqg_ensemble_load: checkpoint of a different ensemble (systems, size or precision)");
+    const auto parts = checkpointParts(*ens, h.psiElems);
+    uint64_t total = sizeof(h);
+    for (auto& p : parts) total += p.second;
+    if (size != total) return fail(CQG_E_INVALID, "cqg_ensemble_load: checkpoint size mismatch");
+    ck(cudaStreamSynchronize(ens->stream), "cudaStreamSynchronize");
+    const char* in = static_cast<const char*>(buf) + sizeof(h);
+    for (auto& p : parts) {
+      ck(cudaMemcpy(p.first, in, p.second, cudaMemcpyHostToDevice), "cudaMemcpy(checkpoint)");
+      in += p.second;
+    }
+    return CQG_OK;
+  });
+}
+
 int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap) {
   if (!ens || !n_groups || (cap > 0 && !plan)) return fail(CQG_E_INVALID, "cqg_ensemble_plan: null argument");
   *n_groups = int32_t(ens->groups.size());
@@ -921,13 +1016,15 @@ int cqg_ensemble_get_counters(const cqg_ensemble* ens, uint64_t* counters) {
   });
 }
 
-int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_norm_dev) {
+int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_tolerance_overshoot,
+                                   double* max_norm_dev) {
   return guardedCuda([&] {
     if (!ens) return fail(CQG_E_INVALID, "null ensemble");
     std::vector<double> m(3 * ens->nTraj);
     ck(cudaMemcpy(m.data(), ens->td.maxima, m.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
     for (int64_t i = 0; i < ens->nTraj; ++i) {
       if (max_overshoot) max_overshoot[i] = m[3 * i];
+      if (max_tolerance_overshoot) max_tolerance_overshoot[i] = m[3 * i + 1];
       if (max_norm_dev) max_norm_dev[i] = m[3 * i + 2];
     }
     return CQG_OK;

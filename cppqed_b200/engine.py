@@ -227,11 +227,15 @@ class Ensemble:
         return c
 
     def logger_maxima(self):
+        """Per trajectory: maximal dpLimit overshoot, maximal dpTolerance overshoot, maximal
+        deviation of the norm from 1 (mcwf::Logger)."""
         a = np.zeros(self.n_traj)
         b = np.zeros(self.n_traj)
+        c = np.zeros(self.n_traj)
         P = C.POINTER(C.c_double)
-        check(lib().cqg_ensemble_get_logger_maxima(self._h, a.ctypes.data_as(P), b.ctypes.data_as(P)))
-        return a, b
+        check(lib().cqg_ensemble_get_logger_maxima(self._h, a.ctypes.data_as(P), b.ctypes.data_as(P),
+                                                   c.ctypes.data_as(P)))
+        return a, b, c
 
     def jumps(self, i, cap=64):
         t = np.zeros(cap)
@@ -252,6 +256,17 @@ class Ensemble:
         r = C.c_double()
         check(lib().cqg_ensemble_last_kernel_ms(self._h, C.byref(k), C.byref(r)))
         return k.value, r.value
+
+    def save(self):
+        """Checkpoint of every trajectory (bytes), see cqg_ensemble_save."""
+        n = C.c_uint64()
+        check(lib().cqg_ensemble_save(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(lib().cqg_ensemble_save(self._h, buf, n.value, C.byref(n)))
+        return buf.raw
+
+    def load(self, state):
+        check(lib().cqg_ensemble_load(self._h, C.c_char_p(state), len(state)))
 
     def plan(self):
         """Kernel groups: list of dicts (kind, E, smax, threads, count)."""

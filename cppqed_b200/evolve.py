@@ -11,6 +11,10 @@ Mirrors ``evolve(psi, sys, pe)`` (high/Evolution_.h:174-209) dispatching to
 
 Each streamed row is ``[t, dtDid, averages...]`` after ``Averaged::process``.  The
 master equation (``--evol master``) is not run on the device.
+
+``ensemble_log`` writes the end-of-run log of an ensemble (mcwf::EnsembleLogger::stream,
+MCWF_TrajectoryLogger.cc:79-121) and ``trajectory_log`` that of one trajectory
+(mcwf::Logger::onEnd, :19-33), from the device's logger counters and jump records.
 """
 import numpy as np
 
@@ -26,9 +30,11 @@ def _row(model, t, sums, n_traj):
     return row
 
 
-def evolve(script, args=(), rng=None, precision=None, n_traj=None):
+def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None):
     """Runs the script's system as the reference's trajectory::run would.
 
+    resume: a checkpoint (Ensemble.save) to continue from, as --continue does; the
+    continued run streams no initial row (Trajectory.h:585).
     Returns (rows, ensemble, model); rows has one line per stream."""
     model = Model(script, args)
     rp = model.run_pars()
@@ -47,7 +53,11 @@ def evolve(script, args=(), rng=None, precision=None, n_traj=None):
     def front_time():
         return ens.times()[0][0]
 
-    rows = [_row(model, 0.0, ens.steps(0, rp.T), n_traj)]
+    if resume is not None:
+        ens.load(resume)
+        rows = []
+    else:
+        rows = [_row(model, 0.0, ens.steps(0, rp.T), n_traj)]
     if rp.evol == A.EVOL_SINGLE and rp.dc:
         T = rp.T
         while front_time() < T:
@@ -81,3 +91,76 @@ def evolve(script, args=(), rng=None, precision=None, n_traj=None):
                 t = t + delta
                 rows.append(_row(model, t, sums[0], n_traj))
     return np.array(rows), ens, model
+
+
+def ensemble_log_values(ens):
+    """The numbers of mcwf::EnsembleLogger::stream: averages over the trajectories of the
+    accepted steps, dpLimit and dpTolerance overshoots and jumps; maxima over the
+    trajectories of the overshoots and of |norm - 1|."""
+    c = ens.counters().astype(np.float64)
+    mo, mt, mn = ens.logger_maxima()
+    return {"average_steps": c[:, 0].mean(), "average_overshot": c[:, 4].mean(), "max_overshoot": mo.max(),
+            "average_tolerance_overshot": c[:, 5].mean(), "max_tolerance_overshoot": mt.max(),
+            "max_norm_deviation": mn.max(), "average_jumps": c[:, 6].mean(), "total_jumps": int(c[:, 6].sum())}
+
+
+def _density(samples, n_bins):
+    """Histogram of boost::accumulators' density feature with the whole sample as its
+    cache: n_bins equal bins between the sample's minimum and maximum, one underflow and one
+    overflow bin in front and behind; each bin as (lower edge, fraction of the samples)."""
+    lo, hi = min(samples), max(samples)
+    width = (hi - lo) / n_bins
+    edges = [lo + (i - 1) * width for i in range(n_bins + 2)]
+    counts = [0] * (n_bins + 2)
+    for x in samples:
+        if x < edges[1]:
+            counts[0] += 1
+        elif x >= edges[n_bins + 1]:
+            counts[n_bins + 1] += 1
+        else:
+            k = 1
+            while k < n_bins + 1 and x >= edges[k + 1]:
+                k += 1
+            counts[k] += 1
+    return [(edges[i], counts[i] / len(samples)) for i in range(n_bins + 2)]
+
+
+def ensemble_log(ens, n_bins=0, n_jumps_per_bin=50):
+    """Text of mcwf::EnsembleLogger::stream (numbers in the stream's default 6 digits).  The
+    histogram is built from the jump records the device keeps (the last 64 of each
+    trajectory)."""
+    v = ensemble_log_values(ens)
+    g = "{:.6g}".format
+    out = ["", "Average number of total steps: " + g(v["average_steps"]), "",
+           "On average, dpLimit overshot: %s times, maximal overshoot: %s" % (g(v["average_overshot"]),
+                                                                             g(v["max_overshoot"])),
+           "On average, dpTolerance overshot: %s times, maximal overshoot: %s" % (
+               g(v["average_tolerance_overshot"]), g(v["max_tolerance_overshoot"])), "",
+           "Maximal deviation of norm from 1: " + g(v["max_norm_deviation"])]
+    total = v["total_jumps"]
+    if not n_bins and total < 2 * n_jumps_per_bin:
+        out += ["", "Too few jumps for a histogram"]
+    else:
+        bins = n_bins if n_bins else total // n_jumps_per_bin
+        times = []
+        for i in range(ens.n_traj):
+            t, _ = ens.jumps(i, 1 << 20)
+            times.extend(t.tolist())
+        out += ["", "Histogram of jumps. Number of bins=%d" % (bins + 2)]
+        out += ["%s\t%s" % (g(a), g(b)) for a, b in _density(times, bins)]
+    out += ["", "Average number of total jumps: " + g(total / ens.n_traj)]
+    return "\n".join(out) + "\n"
+
+
+def trajectory_log(ens, i=0):
+    """Text of mcwf::Logger::onEnd for trajectory i (log level > 0)."""
+    c = ens.counters()[i]
+    mo, mt, mn = ens.logger_maxima()
+    t, l = ens.jumps(i, 1 << 20)
+    g = "{:.6g}".format
+    out = ["", "Total number of MCWF steps: %d" % c[0], "",
+           "dpLimit overshot: %d times, maximal overshoot: %s" % (c[4], g(mo[i])),
+           "dpTolerance overshot: %d times, maximal overshoot: %s" % (c[5], g(mt[i])), "",
+           "Maximal deviation of norm from 1: " + g(mn[i]), "", "MCWF Trajectory:"]
+    out += ["%s\t%d" % (g(a), b) for a, b in zip(t, l)]
+    return "\n".join(out) + "\n\n"

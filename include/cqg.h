@@ -217,8 +217,10 @@ int cqg_ensemble_get_times(const cqg_ensemble* ens, double* t, double* dt_did, d
  * 3 RHS evaluations, 4 dpLimit overshoots, 5 step-backs, 6 jumps, 7 status bits. */
 int cqg_ensemble_get_counters(const cqg_ensemble* ens, uint64_t* counters);
 
-/* Max overshoot (MCWF logger) and max |norm-1| per trajectory. */
-int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_norm_dev);
+/* Per trajectory (any pointer may be NULL): maximal dpLimit overshoot, maximal dpTolerance
+ * overshoot and maximal |norm - 1| (mcwf::Logger, MCWF_TrajectoryLogger.cc:37-56). */
+int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoot, double* max_tolerance_overshoot,
+                                   double* max_norm_dev);
 
 /* Jump record ring per trajectory: up to `cap` (time, lindblad) pairs of the
  * most recent jumps (MCWF logger jump list, MCWF_TrajectoryLogger.cc:42-75). */
@@ -240,6 +242,17 @@ int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, doub
  * plan: kind (0 = warp per trajectory, 1 = CTA per trajectory), rows per lane E (warp
  * kind), off-diagonal slot bound, CTA threads, trajectories in the group. */
 int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap);
+
+/* ---- checkpoint / continuation -------------------------------------------
+ * The role of the reference's trajectory state archive (trajectory::writeViaSStream /
+ * readViaSStream, Trajectory.h:353-424, MCWF_Trajectory.h:134-147, used by --continue),
+ * in this library's own binary layout: every trajectory's state vector, t, t0, dtTry,
+ * dtDid, random stream, logger counters and maxima, status and jump records.
+ * cqg_ensemble_save with buf == NULL or cap too small only reports the size.
+ * cqg_ensemble_load requires an ensemble created over the same systems, trajectory
+ * count and precision; the continued run is bit-identical to an uninterrupted one.      */
+int cqg_ensemble_save(const cqg_ensemble* ens, void* buf, uint64_t cap, uint64_t* size);
+int cqg_ensemble_load(cqg_ensemble* ens, const void* buf, uint64_t size);
 
 /* ---- request server ------------------------------------------------------
  * Continuous batching of ensemble requests (no reference counterpart: C++QED runs one

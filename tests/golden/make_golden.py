@@ -2,7 +2,9 @@
 
 Reads Testing/expected/run_<name> (C++QED v2.120, written by CPPQEDscripts with the
 command lines of Testing/run/testdriver.conf) and stores, per run, the command line,
-the streamed rows (time, dtDid, averages) and the pcg64 engine state serialised in
+the streamed rows (time, dtDid, averages), the numbers of the end-of-run ensemble log
+(mcwf::EnsembleLogger::stream: average steps, dpLimit / dpTolerance overshoots with their
+maxima, maximal norm deviation, average jumps) and the pcg64 engine state serialised in
 the first archive of the matching .state file (the engine right after seeding).
 Run once where the reference tree is available:
 
@@ -20,16 +22,34 @@ RUNS += ["run_1particle1mode_%s_%s" % (m, e) for m in ("dc", "dt", "ndt", "ndt_c
 RUNS += ["run_Ring_%s_%s" % (m, e) for m in ("dc", "dt", "ndt") for e in ("single", "ensemble", "master")]
 
 
+LOG_PATTERNS = {
+    "average_steps": r"Average number of total steps: (\S+)",
+    "average_overshot": r"On average, dpLimit overshot: (\S+) times",
+    "max_overshoot": r"dpLimit overshot: \S+ times, maximal overshoot: (\S+)",
+    "average_tolerance_overshot": r"On average, dpTolerance overshot: (\S+) times",
+    "max_tolerance_overshoot": r"dpTolerance overshot: \S+ times, maximal overshoot: (\S+)",
+    "max_norm_deviation": r"Maximal deviation of norm from 1: (\S+)",
+    "average_jumps": r"Average number of total jumps: (\S+)",
+}
+
+
 def parse(path):
-    cmd, rows = None, []
+    cmd, rows, log = None, [], {}
     for line in open(path):
         if line.startswith("#"):
             if cmd is None and line.strip() != "#":
                 cmd = line[1:].strip()
+            if rows:
+                for key, pat in LOG_PATTERNS.items():
+                    m = re.search(pat, line)
+                    if m:
+                        log[key] = float(m.group(1))
+                if "Too few jumps for a histogram" in line:
+                    log["histogram"] = False
             continue
         if line.strip():
             rows.append([float(x) for x in line.split()])
-    return cmd, rows
+    return cmd, rows, log
 
 
 def pcg_state(path):
@@ -47,13 +67,15 @@ def main(ref):
         p = os.path.join(exp, r)
         if not os.path.exists(p):
             continue
-        cmd, rows = parse(p)
+        cmd, rows, log = parse(p)
         args = cmd.split()[1:]
         if "--o" in args:
             i = args.index("--o")
             del args[i:i + 2]
         out[r] = {"script": os.path.basename(cmd.split()[0]), "args": args, "rows": rows,
                   "pcg64_first_archive": pcg_state(p + ".state")}
+        if log:
+            out[r]["ensemble_log"] = log
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_runs.json")
     json.dump(out, open(dst, "w"), indent=0)
     print("wrote", dst, len(out), "runs")
