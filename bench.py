@@ -284,23 +284,20 @@ def run_ours(args, rank, world, dev):
 
     import cppqed_b200 as cqg
     from cppqed_b200 import _abi as A
+    from cppqed_b200 import sharding
 
     script, sargs, n_traj, Dt = WORKLOADS[args.workload]
     model = cqg.Model(script, sargs)
     pars = model.run_pars().mcwf
     pars.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
     pars.precision = A.FP64 if args.precision == "fp64" else A.FP32
-    pars.prng_stream = 1 + rank * n_traj
+    pars.prng_stream = sharding.first_stream(1, n_traj, rank)
     system = cqg.System(model.desc)
     psi0 = model.initial_state()
     ens = cqg.Ensemble(system, psi0, n_traj, pars)
 
     def allreduce(x):
-        if world > 1:
-            t = torch.tensor(x, dtype=torch.float64, device="cuda")
-            torch.distributed.all_reduce(t)
-            return t.cpu().numpy()
-        return x
+        return sharding.allreduce_sum(x, world)
 
     for _ in range(args.warmup):
         allreduce(ens.run(Dt, 1))
@@ -325,11 +322,7 @@ def run_ours(args, rank, world, dev):
     d = (c1.astype(np.int64) - c0.astype(np.int64)).sum(axis=0)
     steps_local, attempts_local, rhs_local = int(d[0]), int(d[1]), int(d[3])
     tot = allreduce(np.array([steps_local, attempts_local, rhs_local], dtype=np.float64))
-    tmax = allreduce(np.array([run_ms, kernel_ms])) if world == 1 else None
-    if world > 1:
-        t = torch.tensor([run_ms, kernel_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tmax = t.cpu().numpy()
+    tmax = sharding.max_over_ranks([run_ms, kernel_ms], world)
     run_ms_max, kernel_ms_max = float(tmax[0]), float(tmax[1])
     steps_total = float(tot[0])
     value = steps_total / (run_ms_max * 1e-3)
@@ -347,10 +340,7 @@ def run_ours(args, rank, world, dev):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_tot = allreduce(np.array([e2e_steps, e2e_s], dtype=np.float64))
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = float(sharding.max_over_ranks([e2e_s], world)[0])
     e2e_value = float(e2e_tot[0]) / e2e_s
     h2d = n_traj * model.dim * 16 + n_traj * (8 * 4 + 32 + 64)
     d2h = (model.n_avr + 1) * 8 + 4
