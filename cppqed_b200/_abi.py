@@ -154,6 +154,13 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_load": (C.c_int, [_P, C.c_void_p, C.c_uint64]),
     "cqg_ensemble_plan": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.c_int32]),
     "cqg_probe_fma_peaks": (C.c_int, [_DP, _DP]),
+    "cqg_master_create": (C.c_int, [_P, _CP, C.POINTER(cqg_mcwf_pars), C.POINTER(_P)]),
+    "cqg_master_run": (C.c_int, [_P, C.c_double, C.c_int32, _DP]),
+    "cqg_master_steps": (C.c_int, [_P, C.c_int32, C.c_double, _DP]),
+    "cqg_master_averages": (C.c_int, [_P, _DP]),
+    "cqg_master_get_rho": (C.c_int, [_P, _CP]),
+    "cqg_master_get_times": (C.c_int, [_P, _DP, _DP, _DP]),
+    "cqg_master_destroy": (C.c_int, [_P]),
     "cqg_server_pars_default": (None, [C.POINTER(cqg_server_pars)]),
     "cqg_server_create": (C.c_int, [C.POINTER(cqg_server_pars), C.POINTER(_P)]),
     "cqg_server_submit": (C.c_int, [_P, _P, _CP, C.c_int64, C.c_double, C.c_double, C.c_uint64,

@@ -18,10 +18,10 @@ LIB = os.path.join(LIBDIR, "libcqg.so")
 
 HOST_SOURCES = ["host/tridiagonal.cpp", "host/elements.cpp", "host/model.cpp", "host/pars.cpp",
                 "host/scripts.cpp", "host/errors.cpp", "host/api_model.cpp", "host/lowering.cpp"]
-CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu", "cuda/kernels_block.cu", "cuda/apply.cu", "cuda/server.cu"]
+CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu", "cuda/kernels_block.cu", "cuda/apply.cu", "cuda/server.cu", "cuda/master.cu"]
 # the kernel instantiations: one object per (precision, rows per lane)
 KERNEL_INSTANCES = [(r, e) for r in ("double", "float") for e in (1, 2, 3, 4)]
-HEADERS = ["cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/mcwf_block.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
+HEADERS = ["cuda/engine_internal.cuh", "cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/mcwf_block.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
            "host/elements.hpp", "host/tridiagonal.hpp", "host/pars.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

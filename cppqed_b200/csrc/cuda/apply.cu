@@ -24,6 +24,7 @@
 
 #include "../host/errors.hpp"
 #include "cqg.h"
+#include "engine_internal.cuh"
 #include "mcwf_kernel.cuh"
 
 namespace cqg {
@@ -294,6 +295,35 @@ cudaError_t launchElement(const SysDev& sd, const double2* psi, double2* dpsi, l
 
 }  // namespace
 
+namespace cqg {
+namespace engine {
+
+cudaError_t applyHamiltonian(const SysDev& sd, const double2* p, double2* q, long long nStates, double tau,
+                             cudaStream_t st, int nSM) {
+  StagedGeom g{};
+  size_t smemBytes = 0;
+  if (sd.S <= 4 && stagedGeometry(sd.D, nStates, g, smemBytes)) {
+    switch (sd.S) {
+      case 0: return launchStaged<0>(sd, p, q, g, smemBytes, tau, st, nSM);
+      case 1: return launchStaged<1>(sd, p, q, g, smemBytes, tau, st, nSM);
+      case 2: return launchStaged<2>(sd, p, q, g, smemBytes, tau, st, nSM);
+      case 3: return launchStaged<3>(sd, p, q, g, smemBytes, tau, st, nSM);
+      default: return launchStaged<4>(sd, p, q, g, smemBytes, tau, st, nSM);
+    }
+  }
+  switch (sd.S) {
+    case 0: return launchElement<0>(sd, p, q, nStates, tau, st, nSM);
+    case 1: return launchElement<1>(sd, p, q, nStates, tau, st, nSM);
+    case 2: return launchElement<2>(sd, p, q, nStates, tau, st, nSM);
+    case 3: return launchElement<3>(sd, p, q, nStates, tau, st, nSM);
+    case 4: return launchElement<4>(sd, p, q, nStates, tau, st, nSM);
+    default: return launchElement<-1>(sd, p, q, nStates, tau, st, nSM);
+  }
+}
+
+}  // namespace engine
+}  // namespace cqg
+
 extern "C" int cqg_system_apply_hamiltonian(const cqg_system* sys, const cqg_complex* psi, cqg_complex* dpsi,
                                             int64_t n_states, double tau, void* stream) {
   if (!sys || !psi || !dpsi || n_states < 1)
@@ -307,29 +337,8 @@ extern "C" int cqg_system_apply_hamiltonian(const cqg_system* sys, const cqg_com
     return fail(CQG_E_INVALID, "cqg_system_apply_hamiltonian: the current device is not the system's device");
   if ((reinterpret_cast<uintptr_t>(psi) | reinterpret_cast<uintptr_t>(dpsi)) % 16 != 0)
     return fail(CQG_E_INVALID, "cqg_system_apply_hamiltonian: psi and dpsi must be 16-byte aligned");
-  const double2* p = reinterpret_cast<const double2*>(psi);
-  double2* q = reinterpret_cast<double2*>(dpsi);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  StagedGeom g{};
-  size_t smemBytes = 0;
-  if (sd->S <= 4 && stagedGeometry(sd->D, n_states, g, smemBytes)) {
-    switch (sd->S) {
-      case 0: err = launchStaged<0>(*sd, p, q, g, smemBytes, tau, st, nSM); break;
-      case 1: err = launchStaged<1>(*sd, p, q, g, smemBytes, tau, st, nSM); break;
-      case 2: err = launchStaged<2>(*sd, p, q, g, smemBytes, tau, st, nSM); break;
-      case 3: err = launchStaged<3>(*sd, p, q, g, smemBytes, tau, st, nSM); break;
-      default: err = launchStaged<4>(*sd, p, q, g, smemBytes, tau, st, nSM); break;
-    }
-  } else {
-    switch (sd->S) {
-      case 0: err = launchElement<0>(*sd, p, q, n_states, tau, st, nSM); break;
-      case 1: err = launchElement<1>(*sd, p, q, n_states, tau, st, nSM); break;
-      case 2: err = launchElement<2>(*sd, p, q, n_states, tau, st, nSM); break;
-      case 3: err = launchElement<3>(*sd, p, q, n_states, tau, st, nSM); break;
-      case 4: err = launchElement<4>(*sd, p, q, n_states, tau, st, nSM); break;
-      default: err = launchElement<-1>(*sd, p, q, n_states, tau, st, nSM); break;
-    }
-  }
+  err = cqg::engine::applyHamiltonian(*sd, reinterpret_cast<const double2*>(psi), reinterpret_cast<double2*>(dpsi),
+                                      n_states, tau, static_cast<cudaStream_t>(stream), nSM);
   if (err != cudaSuccess) return fail(CQG_E_CUDA, std::string("apply launch: ") + cudaGetErrorString(err));
   return CQG_OK;
 }

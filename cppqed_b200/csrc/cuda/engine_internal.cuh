@@ -96,5 +96,10 @@ std::vector<double> hostRates(const LoweredSystem& L, const std::vector<dcomp>& 
 // when the initial step overshoots dpLimit (the logger's overshoot counter).
 double initialDtTry(const cqg_system& s, const std::vector<dcomp>& psi, const cqg_mcwf_pars& p, bool* overshot);
 
+// dpsi_i += (H/i)(tau) psi_i for nStates contiguous states of sd.D elements (16-byte
+// aligned), queued on st: the batched Hamiltonian::addContribution of apply.cu
+cudaError_t applyHamiltonian(const dev::SysDev& sd, const double2* psi, double2* dpsi, long long nStates, double tau,
+                             cudaStream_t st, int nSM);
+
 }  // namespace engine
 }  // namespace cqg

@@ -286,6 +286,48 @@ def probe_fma_peaks():
     return a.value, b.value
 
 
+class Master:
+    """Master equation on the device (cqg_master_*); rho starts as |psi0><psi0|."""
+
+    def __init__(self, system, psi0, pars):
+        self._keep = system
+        self.n_avr = None
+        buf, _keep = to_c(psi0)
+        self.dim = len(psi0)
+        h = C.c_void_p()
+        check(lib().cqg_master_create(system._h, buf, C.byref(pars), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().cqg_master_destroy(self._h)
+            self._h = None
+
+    def _buf(self, rows, n_avr):
+        return np.zeros((rows, n_avr + 1))
+
+    def run(self, Dt, n_intervals, n_avr):
+        """Expectation values (n_avr linear averages, then dtDid) after each interval."""
+        out = self._buf(n_intervals, n_avr)
+        check(lib().cqg_master_run(self._h, float(Dt), int(n_intervals), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def steps(self, n_steps, T, n_avr):
+        out = self._buf(1, n_avr)
+        check(lib().cqg_master_steps(self._h, int(n_steps), float(T), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out[0]
+
+    def rho(self):
+        r = np.zeros((self.dim, self.dim), dtype=np.complex128)
+        check(lib().cqg_master_get_rho(self._h, r.ctypes.data_as(C.POINTER(A.cqg_complex))))
+        return r
+
+    def times(self):
+        t, did, tr = C.c_double(), C.c_double(), C.c_double()
+        check(lib().cqg_master_get_times(self._h, C.byref(t), C.byref(did), C.byref(tr)))
+        return t.value, did.value, tr.value
+
+
 class Server:
     """Continuous-batching request server (cqg_server_*)."""
 

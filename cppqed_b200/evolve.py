@@ -9,8 +9,9 @@ Mirrors ``evolve(psi, sys, pe)`` (high/Evolution_.h:174-209) dispatching to
   dc mode does not apply, StochasticTrajectory.h:193-256); every stream carries the
   ensemble average of the linear observables and the mean dtDid.
 
-Each streamed row is ``[t, dtDid, averages...]`` after ``Averaged::process``.  The
-master equation (``--evol master``) is not run on the device.
+Each streamed row is ``[t, dtDid, averages...]`` after ``Averaged::process``.
+``--evol master`` runs the master equation on the device (cqg_master_*), with the same
+dc / Dt / NDt loops (a Master trajectory has a step, so dc mode applies).
 
 ``ensemble_log`` writes the end-of-run log of an ensemble (mcwf::EnsembleLogger::stream,
 MCWF_TrajectoryLogger.cc:79-121) and ``trajectory_log`` that of one trajectory
@@ -19,7 +20,7 @@ MCWF_TrajectoryLogger.cc:79-121) and ``trajectory_log`` that of one trajectory
 import numpy as np
 
 from . import _abi as A
-from .engine import Ensemble, Model, System
+from .engine import Ensemble, Master, Model, System
 
 
 def _row(model, t, sums, n_traj):
@@ -39,7 +40,7 @@ def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None):
     model = Model(script, args)
     rp = model.run_pars()
     if rp.evol == A.EVOL_MASTER:
-        raise NotImplementedError("the master equation is not run on the device")
+        return _evolve_master(model, rp)
     pars = rp.mcwf
     if rng is not None:
         pars.rng = rng
@@ -164,3 +165,37 @@ def trajectory_log(ens, i=0):
            "Maximal deviation of norm from 1: " + g(mn[i]), "", "MCWF Trajectory:"]
     out += ["%s\t%d" % (g(a), b) for a, b in zip(t, l)]
     return "\n".join(out) + "\n\n"
+
+
+def _evolve_master(model, rp):
+    """trajectory::run of a Master trajectory (Trajectory.h:462-610) on the device."""
+    system = System(model.desc)
+    m = Master(system, model.initial_state(), rp.mcwf)
+    n = model.n_avr
+
+    def row(t, vals):
+        r = np.empty(2 + n)
+        r[0] = t
+        r[1] = vals[n]
+        r[2:] = model.process(np.asarray(vals[:n]))
+        return r
+
+    rows = [row(0.0, m.steps(0, rp.T, n))]
+    if rp.dc:  # dc mode: a row every dc steps until T
+        while m.times()[0] < rp.T:
+            vals = m.steps(rp.dc, rp.T, n)
+            rows.append(row(m.times()[0], vals))
+    elif rp.NDt:  # NDt intervals of Dt
+        t = m.times()[0]
+        for vals in m.run(rp.Dt, int(rp.NDt), n):
+            t = t + rp.Dt
+            rows.append(row(t, vals))
+    else:  # Dt intervals up to T, the last one shortened
+        T, Dt = rp.T, rp.Dt
+        t = m.times()[0]
+        while t < T:
+            delta = min(Dt, T - t)
+            vals = m.run(delta, 1, n)[0]
+            t = t + delta
+            rows.append(row(t, vals))
+    return np.array(rows), m, model

@@ -254,6 +254,25 @@ int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan,
 int cqg_ensemble_save(const cqg_ensemble* ens, void* buf, uint64_t cap, uint64_t* size);
 int cqg_ensemble_load(cqg_ensemble* ens, const void* buf, uint64_t size);
 
+/* ---- master equation ------------------------------------------------------
+ * quantumtrajectory::Master (Master.h:153-208) on the device for the same system:
+ * drho/dt = A rho + (A rho)^+ + sum_m J_m rho J_m^+ (A = H/i), the controlled Cash-Karp
+ * step of the trajectories over all D^2 elements, then U rho U^+ with the exact part and
+ * exact Hermiticity and normalisation.  rho starts as |psi0><psi0|.  Rows are the
+ * expectation values Tr(O rho) of the system's n_avr linear averages followed by dtDid.
+ * Memory: 11 D x D complex128 matrices.                                              */
+typedef struct cqg_master cqg_master;
+int cqg_master_create(const cqg_system* sys, const cqg_complex* psi0, const cqg_mcwf_pars* pars, cqg_master** out);
+/* n_intervals intervals of Dt (ODE steps never cross an interval's end), one row each. */
+int cqg_master_run(cqg_master* m, double Dt, int32_t n_intervals, double* avr_out);
+/* Up to n_steps ODE steps of size T - t (dc mode), then one row (avr_out may be NULL). */
+int cqg_master_steps(cqg_master* m, int32_t n_steps, double T, double* avr_out);
+int cqg_master_averages(cqg_master* m, double* avr_out);
+/* rho in row-major order (D x D complex128). */
+int cqg_master_get_rho(const cqg_master* m, cqg_complex* rho);
+int cqg_master_get_times(const cqg_master* m, double* t, double* dt_did, double* dt_try);
+int cqg_master_destroy(cqg_master* m);
+
 /* ---- request server ------------------------------------------------------
  * Continuous batching of ensemble requests (no reference counterpart: C++QED runs one
  * ensemble at a time, Ensemble::advance, StochasticTrajectory.h:220-245).  A request is a

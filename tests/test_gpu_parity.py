@@ -510,3 +510,35 @@ def test_checkpoint_of_another_ensemble_is_refused(gpu):
     with pytest.raises(gpu.EngineError) as e:
         e2.load(e1.save())
     assert e.value.code == A.CQG_E_INVALID
+
+
+# ---- master equation on the device ----
+
+@pytest.mark.parametrize("run", ["run_PTLA_CPPQED_%s_master" % m for m in ("dc", "dt", "ndt")] +
+                         ["run_1particle1mode_%s_master" % m
+                          for m in ("dc", "dt", "ndt", "ndt_conf2", "ndt_conf3", "ndt_conf4")] +
+                         ["run_Ring_%s_master" % m for m in ("dc", "dt", "ndt")])
+def test_master_golden_on_device(gpu, golden, run):
+    """quantumtrajectory::Master on the device reproduces the reference's golden master
+    runs (np.allclose, as testdriver.py)."""
+    g = golden[run]
+    rows, _, _ = gpu.evolve(g["script"], g["args"])
+    ref = np.array(g["rows"])
+    assert rows.shape == ref.shape
+    assert np.allclose(rows, ref)
+
+
+def test_master_matches_oracle_master(gpu, oracle):
+    """Qubit-mode 2 x 40 (D = 80, a 6400-element rho, two jump operators): device and oracle
+    master equations agree row by row on the same Dt grid."""
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    ref = _master_rows(oracle, model, 0.5, 0.1)
+    sysd = gpu.System(model.desc)
+    m = gpu.Master(sysd, model.initial_state(), model.run_pars().mcwf)
+    got = m.run(0.1, 5, model.n_avr)
+    for k in range(5):
+        vals = model.process(got[k][:model.n_avr])
+        assert np.allclose(vals, ref[k + 1][2:], rtol=1e-8, atol=1e-10), k
+    rho = m.rho()
+    assert np.allclose(rho, rho.conj().T, atol=1e-14)
+    assert abs(np.trace(rho).real - 1) < 1e-12
