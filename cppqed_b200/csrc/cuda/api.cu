@@ -240,14 +240,14 @@ using KernelFn = void (*)(dev::TrajDev, dev::RunArgs);
 
 namespace cqg {
 namespace dev {
-KernelFn pick_double_e1(int smax);
-KernelFn pick_double_e2(int smax);
-KernelFn pick_double_e3(int smax);
-KernelFn pick_double_e4(int smax);
-KernelFn pick_float_e1(int smax);
-KernelFn pick_float_e3(int smax);
-KernelFn pick_float_e2(int smax);
-KernelFn pick_float_e4(int smax);
+KernelFn pick_double_e1(int smax, bool ip);
+KernelFn pick_double_e2(int smax, bool ip);
+KernelFn pick_double_e3(int smax, bool ip);
+KernelFn pick_double_e4(int smax, bool ip);
+KernelFn pick_float_e1(int smax, bool ip);
+KernelFn pick_float_e3(int smax, bool ip);
+KernelFn pick_float_e2(int smax, bool ip);
+KernelFn pick_float_e4(int smax, bool ip);
 }  // namespace dev
 }  // namespace cqg
 
@@ -258,7 +258,7 @@ namespace {
 namespace cqg {
 namespace dev {
 using BlockKernelFn = void (*)(TrajDev, RunArgs, BlockScratch, int);
-BlockKernelFn pick_block(bool fp64);
+BlockKernelFn pick_block(bool fp64, bool ip);
 }  // namespace dev
 }  // namespace cqg
 
@@ -268,16 +268,16 @@ namespace {
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
                  const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars);
 
-KernelFn pickKernel(bool fp64, int E, int SMAX) {
+KernelFn pickKernel(bool fp64, int E, int SMAX, bool ip) {
   if (fp64)
-    return E == 1 ? dev::pick_double_e1(SMAX)
-         : E == 2 ? dev::pick_double_e2(SMAX)
-         : E == 3 ? dev::pick_double_e3(SMAX)
-                  : dev::pick_double_e4(SMAX);
-  return E == 1 ? dev::pick_float_e1(SMAX)
-       : E == 2 ? dev::pick_float_e2(SMAX)
-       : E == 3 ? dev::pick_float_e3(SMAX)
-                : dev::pick_float_e4(SMAX);
+    return E == 1 ? dev::pick_double_e1(SMAX, ip)
+         : E == 2 ? dev::pick_double_e2(SMAX, ip)
+         : E == 3 ? dev::pick_double_e3(SMAX, ip)
+                  : dev::pick_double_e4(SMAX, ip);
+  return E == 1 ? dev::pick_float_e1(SMAX, ip)
+       : E == 2 ? dev::pick_float_e2(SMAX, ip)
+       : E == 3 ? dev::pick_float_e3(SMAX, ip)
+                : dev::pick_float_e4(SMAX, ip);
 }
 
 __global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, int nAvrStride, int nAvr,
@@ -452,6 +452,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       const cqg_system* s = systems[e->sysIdx[order[k]]];
       g.Dmax = std::max<int>(g.Dmax, int(s->L.D));
       g.smax = std::max(g.smax, s->sd.S);
+      g.anyFreq |= s->sd.hasFreq != 0;
     }
     g.count = k - g.first;
     e->groups.push_back(g);
@@ -482,9 +483,12 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
                  cudaStream_t st) {
   dev::TrajDev tdArg = td;
   if (g.kind == 0) {
-    KernelFn fn = pickKernel(fp64, g.E, g.smax);
+    KernelFn fn = pickKernel(fp64, g.E, g.smax, g.anyFreq);
     const int warps = g.threads / 32;
-    const size_t smem = size_t(warps) * 3 * 32 * g.E * elemBytes + size_t(warps) * sizeof(dev::WarpScratch);
+    // stage vectors, warp scratch, and for interaction-picture systems the phase cache
+    ra.phaseCache = g.anyFreq ? 1 : 0;
+    const size_t smem = size_t(warps) * 3 * 32 * g.E * elemBytes + size_t(warps) * sizeof(dev::WarpScratch) +
+                        (g.anyFreq ? size_t(warps) * warpSlotInstance(g.smax) * 32 * g.E * sizeof(double2) : 0);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -498,7 +502,7 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
   } else {
     // one CTA per trajectory: stage vectors in shared memory, stage derivatives in a
     // per-CTA scratch slab
-    dev::BlockKernelFn fn = dev::pick_block(fp64);
+    dev::BlockKernelFn fn = dev::pick_block(fp64, g.anyFreq);
     int smemD = g.Dmax;
     const size_t smem = 2 * size_t(smemD) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),

@@ -73,6 +73,7 @@ struct KernelGroup {
   int E = 0;        // warp kind: rows per lane
   int smax = 0;     // off-diagonal slots per row (max over the group's systems)
   int Dmax = 0;
+  bool anyFreq = false;  // some system of the group has interaction-picture frequencies
   int threads = 0;  // CTA size
   int64_t first = 0, count = 0;
   cudaStream_t stream = nullptr;
@@ -82,6 +83,9 @@ struct KernelGroup {
 };
 
 inline int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
+
+// the off-diagonal slot bound of the warp kernel instance that serves smax slots
+inline int warpSlotInstance(int smax) { return smax <= 2 ? 2 : smax <= 4 ? 4 : 8; }
 
 // One persistent launch of group g over td on stream st (ra.order / nTasks / queue set by
 // the caller); allocates or grows the group's block-kernel scratch.

@@ -6,8 +6,9 @@ namespace dev {
 
 using BlockKernelFn = void (*)(TrajDev, RunArgs, BlockScratch, int);
 
-BlockKernelFn pick_block(bool fp64) {
-  return fp64 ? &mcwfBlockKernel<double> : &mcwfBlockKernel<float>;
+BlockKernelFn pick_block(bool fp64, bool ip) {
+  if (ip) return fp64 ? &mcwfBlockKernel<double, true> : &mcwfBlockKernel<float, true>;
+  return fp64 ? &mcwfBlockKernel<double, false> : &mcwfBlockKernel<float, false>;
 }
 
 }  // namespace dev

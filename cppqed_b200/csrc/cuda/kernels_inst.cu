@@ -1,6 +1,6 @@
 // Explicit instantiation of the fused MCWF warp kernel for one (precision, rows per
 // lane) pair; the build compiles this file once per pair (-DCQG_REAL, -DCQG_E) so the
-// instances compile in parallel.  Exposes cqg_pick_<real>_e<E>(SMAX).
+// instances compile in parallel.  Exposes pick_<real>_e<E>(SMAX, interaction picture).
 #include "mcwf_kernel.cuh"
 
 #ifndef CQG_REAL
@@ -18,10 +18,15 @@ namespace dev {
 
 using KernelFn = void (*)(TrajDev, RunArgs);
 
-KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax) {
-  if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2>;
-  if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4>;
-  return &mcwfWarpKernel<CQG_REAL, CQG_E, 8>;
+KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax, bool ip) {
+  if (ip) {
+    if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, true>;
+    if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, true>;
+    return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, true>;
+  }
+  if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, false>;
+  if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, false>;
+  return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, false>;
 }
 
 }  // namespace dev

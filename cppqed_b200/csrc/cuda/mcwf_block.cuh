@@ -59,7 +59,9 @@ __device__ __forceinline__ double blockMax(double v, double* red) {
   return m;
 }
 
-template <typename R>
+// IP: the instance serves interaction-picture systems; the IP = false instance has no
+// phase code.
+template <typename R, bool IP>
 struct BlockWorker {
   using C2 = typename CT<R>::T;
   static constexpr int NR = MAX_JUMPS + 1;
@@ -91,17 +93,20 @@ struct BlockWorker {
   __device__ __forceinline__ C2* cache() const { return vec + 7 * stride; }
 
   // out = (H/i) y, y in shared memory
+  // out = (H/i) y at picture time tau, y in shared memory
   __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
     ++nRhs;
     for (int r = threadIdx.x; r < D; r += blockDim.x) {
       C2 acc = cmul(diag[r], ys[r]);
       for (int s = 0; s < S; ++s) {
         C2 c = __ldg(&val[s * D + r]);
-        if (hasFreq) {
-          const double2 f = __ldg(&freq[s * D + r]);
-          if (f.x != 0. || f.y != 0.) {
-            const double2 ph = cexpScaled(tau, f);
-            c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+        if constexpr (IP) {
+          if (hasFreq && tau != 0.) {  // exp(0 f) = 1 exactly
+            const double2 f = __ldg(&freq[s * D + r]);
+            if (f.x != 0. || f.y != 0.) {
+              const double2 ph = cexpScaled(tau, f);
+              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+            }
           }
         }
         acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
@@ -461,7 +466,7 @@ struct BlockWorker {
 
 // Dynamic shared memory: two stage buffers of `smemD` elements, the reduction scratch,
 // then 8 broadcast words.
-template <typename R>
+template <typename R, bool IP>
 __global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, BlockScratch bsc, int smemD) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char blockSmem[];
@@ -477,7 +482,7 @@ __global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, B
     if (task >= ra.nTasks) return;
     const int ti = ra.order[task];
     const SysDev* s = td.systems + td.sysIdx[ti];
-    BlockWorker<R> w{s, ra};
+    BlockWorker<R, IP> w{s, ra};
     w.D = s->D;
     w.S = s->S;
     w.nJ = s->nJ;

@@ -88,6 +88,23 @@ static __device__ __noinline__ double2 cexpScaled(double tau, double2 f) {
   return make_double2(m * c, m * s);
 }
 
+__device__ __forceinline__ double2 cmulD(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// Interaction-picture phases of the Cash-Karp stages from one exponential per attempt: with
+// E = exp(dt f / 40), stage s (c_s = 1/5, 3/10, 3/5, 1, 7/8) needs exp(c_s dt f) = E^n,
+// n = 8, 12, 24, 40, 35, by repeated squaring (relative error ~ n ulp).
+__device__ __forceinline__ double2 stagePhase(double2 E, int stage) {
+  const double2 e2 = cmulD(E, E), e4 = cmulD(e2, e2), e8 = cmulD(e4, e4);
+  if (stage == 1) return e8;
+  const double2 e12 = cmulD(e8, e4);
+  if (stage == 2) return e12;
+  if (stage == 3) return cmulD(e12, e12);
+  const double2 e16 = cmulD(e8, e8), e32 = cmulD(e16, e16);
+  if (stage == 4) return cmulD(e32, e8);
+  return cmulD(cmulD(e32, e2), E);
+}
+
 // ---- warp reductions -----------------------------------------------------------
 __device__ __forceinline__ unsigned long long globalTimerNs() {
   unsigned long long t;
@@ -209,6 +226,7 @@ struct RunArgs {
   int* queue;
   const int* order;  // the launch's trajectories (a segment of the ensemble's order)
   int nTasks;        // how many
+  int phaseCache;    // shared memory holds a per-warp interaction-picture phase cache
 };
 
 // Cash-Karp tableau (published coefficients)
@@ -230,7 +248,9 @@ struct WarpScratch {
   unsigned long long pcg[4];  // state hi, lo, increment hi, lo (pcg64); word 0 = draw count (philox)
 };
 
-template <typename R, int E, int SMAX>
+// IP: the instance serves interaction-picture systems (rows with frequencies); Schroedinger-
+// picture groups run the IP = false instance, which has no phase code at all.
+template <typename R, int E, int SMAX, bool IP>
 struct Worker {
   using C2 = typename CT<R>::T;
 
@@ -248,6 +268,8 @@ struct Worker {
   C2* buf1;
   C2* cache;
   WarpScratch* ws;
+  double2* phs;  // per-warp phase cache [SMAX][32 E] or null
+  bool phsOn;    // this attempt's stage phases come from phs
 
   // Coefficients live in registers when E * SMAX is small (CREG), else they are
   // re-read per right-hand side through L1 (shared by all trajectories of the system).
@@ -265,8 +287,9 @@ struct Worker {
   double maxOvershoot, maxTolOvershoot, maxNormDev;
   unsigned status;
 
-  __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w)
-      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w) {
+  __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w,
+                                    double2* ph)
+      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w), phs(ph), phsOn(false) {
     D = s->D;
     S = s->S;
     nJ = s->nJ;
@@ -303,7 +326,24 @@ struct Worker {
   }
 
   // out = (H/i) y at picture time tau; y staged through `buf`
-  __device__ __forceinline__ void rhs(const C2 (&y)[E], C2 (&out)[E], double tau, C2* buf) {
+  // E = exp(dt f / 40) of every row and slot for this attempt (t == t0: the stage times are
+  // c_s dt past the picture's reference time)
+  __device__ __forceinline__ void preparePhases(double dt) {
+    const double q = dt / 40.;
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+      if (valid(e)) {
+#pragma unroll
+        for (int s = 0; s < SMAX; ++s)
+          if (s < S) {
+            const double2 f = __ldg(&freq[s * D + row(e)]);
+            phs[s * 32 * E + row(e)] = (f.x != 0. || f.y != 0.) ? cexpScaled(q, f) : make_double2(1., 0.);
+          }
+      }
+  }
+
+  // out = (H/i) y at picture time tau = stage time - t0 (stage 0..5 of the attempt)
+  __device__ __forceinline__ void rhs(const C2 (&y)[E], C2 (&out)[E], double tau, int stage, C2* buf) {
 #pragma unroll
     for (int e = 0; e < E; ++e)
       if (valid(e)) buf[row(e)] = y[e];
@@ -325,11 +365,18 @@ struct Worker {
             c = valid(e) ? __ldg(&val[s * D + r]) : mk<C2>(0, 0);
             cc = __ldg(&col[s * D + r]);
           }
-          if (hasFreq && valid(e)) {
-            const double2 f = __ldg(&freq[s * D + r]);
-            if (f.x != 0. || f.y != 0.) {
-              const double2 ph = cexpScaled(tau, f);
-              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+          if (IP && hasFreq && valid(e)) {
+            if (phsOn) {
+              if (stage) {
+                const double2 ph = stagePhase(phs[s * 32 * E + r], stage);
+                c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+              }
+            } else {
+              const double2 f = __ldg(&freq[s * D + r]);
+              if ((f.x != 0. || f.y != 0.) && tau != 0.) {  // exp(0 f) = 1 exactly
+                const double2 ph = cexpScaled(tau, f);
+                c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+              }
             }
           }
           acc = cfma(c, buf[cc], acc);
@@ -347,7 +394,7 @@ struct Worker {
     if (fabs(dtTry) > fabs(deltaT)) dtTry = deltaT;
     C2 k0[E], k1[E], k2[E], k3[E], k4[E], k5[E], y[E];
     // dxdt at the start is the same for every attempt (Odeint recomputes it per try)
-    rhs(x, k0, t - t0, buf0);
+    rhs(x, k0, t - t0, 0, buf0);
     for (int attempt = 0;; ++attempt) {
       if (attempt >= ra.maxAttempts) {
         status |= 8u;  // CQG_TRAJ_ATTEMPT_LIMIT
@@ -355,31 +402,35 @@ struct Worker {
       }
       ++nAttempts;
       const double dt = dtTry;
+      if constexpr (IP) {
+        phsOn = phs && hasFreq && t == t0;
+        if (phsOn) preparePhases(dt);
+      }
       {
         const R s0 = R(dt * CK::a10);
 #pragma unroll
         for (int e = 0; e < E; ++e) y[e] = axpy(s0, k0[e], x[e]);
       }
-      rhs(y, k1, t + CK::c1 * dt - t0, buf1);
+      rhs(y, k1, t + CK::c1 * dt - t0, 1, buf1);
       {
         const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
 #pragma unroll
         for (int e = 0; e < E; ++e) y[e] = axpy(s1, k1[e], axpy(s0, k0[e], x[e]));
       }
-      rhs(y, k2, t + CK::c2 * dt - t0, buf0);
+      rhs(y, k2, t + CK::c2 * dt - t0, 2, buf0);
       {
         const R s0 = R(dt * CK::a30), s1 = R(dt * CK::a31), s2 = R(dt * CK::a32);
 #pragma unroll
         for (int e = 0; e < E; ++e) y[e] = axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])));
       }
-      rhs(y, k3, t + CK::c3 * dt - t0, buf1);
+      rhs(y, k3, t + CK::c3 * dt - t0, 3, buf1);
       {
         const R s0 = R(dt * CK::a40), s1 = R(dt * CK::a41), s2 = R(dt * CK::a42), s3 = R(dt * CK::a43);
 #pragma unroll
         for (int e = 0; e < E; ++e)
           y[e] = axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e]))));
       }
-      rhs(y, k4, t + CK::c4 * dt - t0, buf0);
+      rhs(y, k4, t + CK::c4 * dt - t0, 4, buf0);
       {
         const R s0 = R(dt * CK::a50), s1 = R(dt * CK::a51), s2 = R(dt * CK::a52), s3 = R(dt * CK::a53),
                 s4 = R(dt * CK::a54);
@@ -387,7 +438,7 @@ struct Worker {
         for (int e = 0; e < E; ++e)
           y[e] = axpy(s4, k4[e], axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])))));
       }
-      rhs(y, k5, t + CK::c5 * dt - t0, buf1);
+      rhs(y, k5, t + CK::c5 * dt - t0, 5, buf1);
       // 5th-order solution, embedded error and the Odeint error norm (max over rows)
       const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
       const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
@@ -749,7 +800,7 @@ struct Worker {
 #define CQG_MIN_BLOCKS 1
 #endif
 
-template <typename R, int E, int SMAX>
+template <typename R, int E, int SMAX, bool IP>
 __global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td, RunArgs ra) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -758,13 +809,19 @@ __global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td
   C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * 3 * DMAX;
   WarpScratch* ws =
       reinterpret_cast<WarpScratch*>(smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) + warp;
+  // optional phase cache after every warp's scratch: [warps][SMAX][DMAX] double2
+  double2* phs = IP && ra.phaseCache ? reinterpret_cast<double2*>(reinterpret_cast<WarpScratch*>(
+                                     smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) +
+                                 blockDim.x / 32) +
+                                     size_t(warp) * SMAX * DMAX
+                               : nullptr;
   while (true) {
     int task = 0;
     if (lane == 0) task = atomicAdd(ra.queue, 1);
     task = __shfl_sync(FULL, task, 0);
     if (task >= ra.nTasks) return;
     const int ti = ra.order[task];
-    Worker<R, E, SMAX> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws);
+    Worker<R, E, SMAX, IP> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws, phs);
     w.run(td, ti);
   }
 }

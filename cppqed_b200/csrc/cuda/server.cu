@@ -305,12 +305,16 @@ void advance(cqg_server& s) {
     g.count = int64_t(v.size());
     g.Dmax = 0;
     g.smax = 0;
+    g.anyFreq = false;
     for (auto& p : v) {
       order.push_back(p.second);
       g.Dmax = std::max<int>(g.Dmax, int(p.first));
     }
     for (auto& req : s.active)
-      if (groupKey(req->sys->L.D, req->sys->sd.S) == key) g.smax = std::max(g.smax, req->sys->sd.S);
+      if (groupKey(req->sys->L.D, req->sys->sd.S) == key) {
+        g.smax = std::max(g.smax, req->sys->sd.S);
+        g.anyFreq |= req->sys->sd.hasFreq != 0;
+      }
     launch.push_back(&g);
   }
   putAsync(s.dOrder, order, st);
