@@ -330,13 +330,19 @@ def run_ours(args, rank, world, dev):
     # end to end through the public API from host buffers: create (upload of the host
     # states), one Dt interval, read-back of the averages, destroy
     e2e_steps = 0
+    phases = np.zeros(4)  # create (host states uploaded), run (one Dt, sums read back), counters, destroy
     t0 = time.perf_counter()
     n_e2e = max(1, min(3, args.steps))
     for _ in range(n_e2e):
+        ta = time.perf_counter()
         e = cqg.Ensemble(system, psi0, n_traj, pars)
+        tb = time.perf_counter()
         allreduce(e.run(Dt, 1))
+        tc = time.perf_counter()
         e2e_steps += int(e.counters()[:, 0].sum())
+        td = time.perf_counter()
         del e
+        phases += [tb - ta, tc - tb, td - tc, time.perf_counter() - td]
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e_tot = allreduce(np.array([e2e_steps, e2e_s], dtype=np.float64))
@@ -355,7 +361,9 @@ def run_ours(args, rank, world, dev):
         "value": value, "ms_per_step": run_ms_max / args.steps, "steps_total": steps_total,
         "attempts_total": float(tot[1]), "rhs_total": float(tot[2]), "kernel_ms": kernel_ms_max,
         "clocks": clocks, "e2e": {"value": e2e_value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": h2d,
-                                  "d2h_bytes_per_step": d2h},
+                                  "d2h_bytes_per_step": d2h, "steps_per_call": e2e_steps / n_e2e,
+                                  "ms_per_call": dict(zip(("create", "run", "counters", "destroy"),
+                                                          [round(1e3 * v / n_e2e, 3) for v in phases]))},
         "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": MCWF_TRAFFIC["bytes"] if (args.workload, args.precision) == (

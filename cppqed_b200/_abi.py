@@ -90,6 +90,8 @@ class cqg_mcwf_pars(C.Structure):
         ("max_attempts", C.c_int32),
         ("autotune", C.c_int32),
         ("cta_threads", C.c_int32),
+        ("cta_shared_vectors", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

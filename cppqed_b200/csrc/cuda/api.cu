@@ -267,6 +267,7 @@ namespace {
 
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
                  const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars);
+bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device);
 
 KernelFn pickKernel(bool fp64, int E, int SMAX, bool ip) {
   if (fp64)
@@ -466,10 +467,14 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     g.threads = pars->cta_threads > 0 ? pars->cta_threads : defaultThreads(g);
     if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 256 : 128))
       return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 256");
+    g.smemVectors = pars->cta_threads > 0 && pars->cta_shared_vectors && sharedVectorsFit(g, e->elemBytes, e->device);
   }
   if (pars->autotune && pars->cta_threads <= 0)
-    for (size_t gi = 0; gi < e->groups.size(); ++gi)
-      e->groups[gi].threads = tunedThreads(*e, gi, systems, nSys, psi0s, psi0Off, *pars);
+    for (size_t gi = 0; gi < e->groups.size(); ++gi) {
+      const int shape = tunedThreads(*e, gi, systems, nSys, psi0s, psi0Off, *pars);
+      e->groups[gi].threads = shape & 0xffff;
+      e->groups[gi].smemVectors = (shape >> 16) != 0;
+    }
   *out = e.release();
   return CQG_OK;
 }
@@ -501,10 +506,10 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
        "kernel launch");
   } else {
     // one CTA per trajectory: stage vectors in shared memory, stage derivatives in a
-    // per-CTA scratch slab
+    // per-CTA scratch slab or, when the group says so, in shared memory too
     dev::BlockKernelFn fn = dev::pick_block(fp64, g.anyFreq);
     int smemD = g.Dmax;
-    const size_t smem = 2 * size_t(smemD) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+    const size_t smem = blockSmemBytes(g.Dmax, elemBytes, g.smemVectors);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -514,17 +519,20 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
     grid = std::max(grid, 1);
     dev::BlockScratch bsc;
     bsc.stride = (g.Dmax + 31) / 32 * 32;
-    const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * elemBytes;
-    if (need > g.scratchBytes) {
-      if (g.scratch) {
-        ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-        cudaFree(g.scratch);
+    bsc.base = nullptr;
+    if (!g.smemVectors) {
+      const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * elemBytes;
+      if (need > g.scratchBytes) {
+        if (g.scratch) {
+          ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+          cudaFree(g.scratch);
+        }
+        g.scratch = nullptr;
+        ck(cudaMalloc(&g.scratch, need), "cudaMalloc(block scratch)");
+        g.scratchBytes = need;
       }
-      g.scratch = nullptr;
-      ck(cudaMalloc(&g.scratch, need), "cudaMalloc(block scratch)");
-      g.scratchBytes = need;
+      bsc.base = g.scratch;
     }
-    bsc.base = g.scratch;
     void* args[] = {&tdArg, &ra, &bsc, &smemD};
     ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(g.threads), args, smem, st),
        "kernel launch");
@@ -612,12 +620,14 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   return CQG_OK;
 }
 
-// Autotuner of the CTA size of a kernel group: the candidates are timed on a sample of
-// the group's trajectories (a scratch ensemble from the same initial states, so the
-// ensemble itself is not advanced) over a fixed number of MCWF steps each, and the fastest
-// is kept.  Results are cached per (device, precision, kernel kind, rows per lane, slot
+// Autotuner of the CTA shape of a kernel group (its size and, for CTA-per-trajectory groups,
+// whether the stage derivatives live in shared memory or in a global scratch slab): the
+// candidates are timed on a sample of the group's trajectories (a scratch ensemble from the
+// same initial states, so the ensemble itself is not advanced) over a fixed number of MCWF
+// steps each, and the fastest is kept.  Results are cached per (device, precision, kernel kind, rows per lane, slot
 // bound, largest dimension) for the life of the process.
-std::vector<int> threadCandidates(const KernelGroup& g) {
+// Candidate shapes, encoded as CTA threads | (shared-memory stage vectors << 16).
+std::vector<int> threadCandidates(const KernelGroup& g, bool vectorsFit) {
   std::vector<int> c;
   if (g.kind == 0) return {64, 128};
   for (int q = 1; q <= 4; ++q) {  // rows per thread
@@ -625,7 +635,17 @@ std::vector<int> threadCandidates(const KernelGroup& g) {
     if (std::find(c.begin(), c.end(), t) == c.end()) c.push_back(t);
   }
   if (std::find(c.begin(), c.end(), 256) == c.end()) c.push_back(256);
+  if (vectorsFit) {
+    const size_t n = c.size();
+    for (size_t k = 0; k < n; ++k) c.push_back(c[k] | (1 << 16));
+  }
   return c;
+}
+
+bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device) {
+  int optin = 0;
+  ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
+  return g.kind == 1 && blockSmemBytes(g.Dmax, elemBytes, true) <= size_t(optin);
 }
 
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
@@ -639,7 +659,7 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
   }
-  const std::vector<int> cands = threadCandidates(g);
+  const std::vector<int> cands = threadCandidates(g, sharedVectorsFit(g, e.elemBytes, e.device));
   int nSM = 0;
   ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e.device), "attribute");
   // enough trajectories to fill the device a couple of times over
@@ -657,7 +677,8 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   }
   cqg_mcwf_pars tp = pars;
   tp.autotune = 0;
-  tp.cta_threads = cands[0];
+  tp.cta_threads = cands[0] & 0xffff;
+  tp.cta_shared_vectors = 0;
   cqg_ensemble* tmp = nullptr;
   if (createEnsemble(systems, nSys, sIdx.data(), psi0s, psi0Off ? sOff.data() : nullptr, n, &tp, &tmp) != CQG_OK)
     return defaultThreads(g);
@@ -671,7 +692,8 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   float bestMs = 0;
   for (int pass = 0; pass < 2; ++pass)  // pass 0 warms up every candidate
     for (int c : cands) {
-      tmp->groups[0].threads = c;
+      tmp->groups[0].threads = c & 0xffff;
+      tmp->groups[0].smemVectors = (c >> 16) != 0;
       ra.nSteps = pass ? 12 : 2;
       if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
       if (pass && (bestMs == 0 || tmp->lastMs < bestMs)) {
@@ -941,7 +963,7 @@ int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan,
   for (int32_t g = 0; g < std::min<int32_t>(cap, *n_groups); ++g) {
     const KernelGroup& k = ens->groups[g];
     int32_t* o = plan + 5 * g;
-    o[0] = k.kind;
+    o[0] = k.kind == 1 && k.smemVectors ? 2 : k.kind;
     o[1] = k.E;
     o[2] = k.smax;
     o[3] = k.threads;

@@ -74,6 +74,7 @@ struct KernelGroup {
   int smax = 0;     // off-diagonal slots per row (max over the group's systems)
   int Dmax = 0;
   bool anyFreq = false;  // some system of the group has interaction-picture frequencies
+  bool smemVectors = false;  // CTA kind: stage derivatives in shared memory instead of scratch
   int threads = 0;  // CTA size
   int64_t first = 0, count = 0;
   cudaStream_t stream = nullptr;
@@ -83,6 +84,14 @@ struct KernelGroup {
 };
 
 inline int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
+
+// Dynamic shared memory of the CTA kernel: two stage vectors of Dmax elements, the reduction
+// scratch and broadcast words, and with shared-memory vectors the kBlockVectors stage
+// derivatives / candidate / cache of ceil32(Dmax) elements each.
+inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors) {
+  const size_t base = 2 * size_t(Dmax) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+  return base + (vectors ? size_t(dev::kBlockVectors) * size_t((Dmax + 31) / 32 * 32) * elemBytes : 0);
+}
 
 // the off-diagonal slot bound of the warp kernel instance that serves smax slots
 inline int warpSlotInstance(int smax) { return smax <= 2 ? 2 : smax <= 4 ? 4 : 8; }

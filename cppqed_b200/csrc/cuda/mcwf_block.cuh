@@ -28,7 +28,8 @@ __constant__ double kBlockA[5][5] = {{1. / 5, 0, 0, 0, 0},
 __constant__ double kBlockC[5] = {1. / 5, 3. / 10, 3. / 5, 1., 7. / 8};
 
 struct BlockScratch {
-  void* base;           // [gridDim.x][kBlockVectors][stride] Real2
+  void* base;           // [gridDim.x][kBlockVectors][stride] Real2, or null: the vectors
+                        // follow the broadcast words in dynamic shared memory
   long long stride;     // elements per vector (>= max D)
 };
 
@@ -495,7 +496,8 @@ __global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, B
     w.val = Tables<R>::val(*s);
     w.diag = Tables<R>::diag(*s);
     w.freq = s->freq;
-    w.vec = reinterpret_cast<C2*>(bsc.base) + size_t(blockIdx.x) * kBlockVectors * bsc.stride;
+    w.vec = bsc.base ? reinterpret_cast<C2*>(bsc.base) + size_t(blockIdx.x) * kBlockVectors * bsc.stride
+                     : reinterpret_cast<C2*>(bcast + 8);
     w.stride = bsc.stride;
     w.ys0 = ys0;
     w.ys1 = ys1;

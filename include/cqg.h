@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 #define CQG_MAX_RANK 8
-#define CQG_ABI_VERSION 2
+#define CQG_ABI_VERSION 3
 
 /* ---- status codes ------------------------------------------------------ */
 #define CQG_OK 0
@@ -139,6 +139,10 @@ typedef struct cqg_mcwf_pars {
                                   sample of its trajectories at creation and keep the fastest
                                   (cached per shape class and device); 0: fixed defaults */
   int32_t cta_threads;         /* > 0: force this CTA size on every group (no tuning) */
+  int32_t cta_shared_vectors;  /* with cta_threads > 0, for CTA-per-trajectory groups: 1 keeps
+                                  the stage derivatives in shared memory (when they fit), 0 in
+                                  a global scratch slab; the autotuner chooses otherwise */
+  int32_t reserved;
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);
@@ -239,7 +243,8 @@ int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, doub
  * trajectories one after another).  Trajectories are grouped by kernel shape, each group
  * one persistent launch per run call, the groups on concurrent streams.  Writes the number
  * of groups to *n_groups and, for the first min(n_groups, cap) groups, five int32 each to
- * plan: kind (0 = warp per trajectory, 1 = CTA per trajectory), rows per lane E (warp
+ * plan: kind (0 = warp per trajectory, 1 = CTA per trajectory with the stage derivatives in
+ * global scratch, 2 = CTA per trajectory with them in shared memory), rows per lane E (warp
  * kind), off-diagonal slot bound, CTA threads, trajectories in the group. */
 int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap);
 

@@ -542,3 +542,24 @@ def test_master_matches_oracle_master(gpu, oracle):
     rho = m.rho()
     assert np.allclose(rho, rho.conj().T, atol=1e-14)
     assert abs(np.trace(rho).real - 1) < 1e-12
+
+
+def test_cta_kernel_shared_memory_vectors_are_bit_identical(gpu):
+    """The CTA-per-trajectory kernel keeps its stage derivatives in a global scratch slab or
+    in shared memory; the arithmetic is the same, so the trajectories are bit-identical."""
+    model = gpu.Model("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30",
+                                        "--etaOpt", "2", "--kappaOpt", "1", "--deltaCOpt", "-1",
+                                        "--kappaMech", "0.1", "--deltaCMech", "-2", "--u", "0.2"])
+    sysd = gpu.System(model.desc)
+    n = 8
+    runs = []
+    for shared in (0, 1):
+        pars = model.run_pars().mcwf
+        pars.cta_threads = 256
+        pars.cta_shared_vectors = shared
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        assert ens.plan()[0]["kind"] == (2 if shared else 1)
+        sums = ens.run(0.2, 2)
+        runs.append((sums, np.stack([ens.state(i, model.dim) for i in range(n)])))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
