@@ -563,3 +563,67 @@ def test_cta_kernel_shared_memory_vectors_are_bit_identical(gpu):
         runs.append((sums, np.stack([ens.state(i, model.dim) for i in range(n)])))
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
+
+
+# ---- special jumps (rate = |J psi|^2) and finite temperature against the master equation ----
+
+def _ensemble_vs_master_z(gpu, oracle, model, n, Dt, K, linear_cols, master_substeps=1):
+    """z-scores of the ensemble means of the linear average columns against the oracle's
+    master equation after each of K intervals, with the standard error from the
+    trajectories' own spread.  master_substeps > 1 runs the master equation on a finer
+    interval grid (its steps never cross an interval's end)."""
+    pars = model.run_pars().mcwf
+    pars.rng = A.RNG_PHILOX
+    sysd = gpu.System(model.desc)
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    master = _master_rows(oracle, model, Dt * K, Dt / master_substeps)[::master_substeps]
+    z = []
+    for k in range(K):
+        ens.run(Dt, 1)
+        per = ens.traj_averages()[:, :model.n_avr]
+        mean = per.mean(axis=0)
+        se = per.std(axis=0, ddof=1) / np.sqrt(n)
+        ref = master[k + 1, 2:]
+        for c in linear_cols:
+            z.append(abs(mean[c] - ref[c]) / max(se[c], 1e-6))
+    return np.array(z)
+
+
+def test_phase_noise_special_jumps_ensemble_vs_master(gpu, oracle):
+    """A qubit with phase noise (LiouvilleanPhaseNoise: both qubit jumps use the special-rate
+    convention, rate = |J psi|^2 computed on the device) coupled to a lossy mode.
+
+    The phase-noise qubit always evolves in the interaction picture, and the reference's
+    Master step applies J rho J^+ untransformed inside an interaction-picture step, which
+    biases it by O(gamma dt) for the non-diagonal loss jump (rho11 at t = 0.25: 0.005886 on
+    a 0.25 grid, 0.006083 on a 0.00025 grid, MCWF 0.00608 +- 0.00002).  The master equation
+    therefore runs on a 100x finer interval grid here."""
+    args = C2_ARGS + ["--gamma_parallel", "0.3"]
+    model = gpu.Model("QbitMode_C++QED", args)
+    z = _ensemble_vs_master_z(gpu, oracle, model, 4096, 0.25, 6, [0, 1, 2, 3, 4, 6, 7], master_substeps=100)
+    assert z.max() < 4.5, z  # 3 sigma with a Bonferroni margin for 42 comparisons
+
+
+def test_phase_noise_trajectories_replay_oracle(gpu, oracle):
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS + ["--gamma_parallel", "0.3"])
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    n = 4
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ens.run(0.5, 2)
+    agree = 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.5, 2)
+        jt, jl = ens.jumps(i, 4096)
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
+    assert agree >= n - 1
+
+
+def test_finite_temperature_mode_ensemble_vs_master(gpu, oracle):
+    """A driven mode at nTh = 0.5: excitation loss and absorption jumps (Mode_.h:220-241)."""
+    model = gpu.Model("PumpedLossyMode_C++QED", C1_ARGS + ["--nTh", "0.5"])
+    z = _ensemble_vs_master_z(gpu, oracle, model, 4096, 0.25, 6, [0, 2, 3])
+    assert z.max() < 4.0, z
