@@ -23,15 +23,18 @@ from . import _abi as A
 from .engine import Ensemble, Master, Model, System
 
 
-def _row(model, t, sums, n_traj):
+def _row(model, t, sums, n_traj, linear=None):
     row = np.empty(2 + model.n_avr)
     row[0] = t
     row[1] = sums[-1] / n_traj
-    row[2:] = model.process(np.asarray(sums[:-1]) / n_traj)
+    avr = np.asarray(sums[:-1]) / n_traj
+    if linear is not None:
+        linear.append(avr.copy())
+    row[2:] = model.process(avr)
     return row
 
 
-def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None):
+def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None, _linear=None):
     """Runs the script's system as the reference's trajectory::run would.
 
     resume: a checkpoint (Ensemble.save) to continue from, as --continue does; the
@@ -58,18 +61,18 @@ def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None):
         ens.load(resume)
         rows = []
     else:
-        rows = [_row(model, 0.0, ens.steps(0, rp.T), n_traj)]
+        rows = [_row(model, 0.0, ens.steps(0, rp.T), n_traj, _linear)]
     if rp.evol == A.EVOL_SINGLE and rp.dc:
         T = rp.T
         while front_time() < T:
             sums = ens.steps(rp.dc, T)
-            rows.append(_row(model, front_time(), sums, n_traj))
+            rows.append(_row(model, front_time(), sums, n_traj, _linear))
     elif rp.NDt:
         t = front_time()
         sums = ens.run(rp.Dt, int(rp.NDt))
         for k in range(int(rp.NDt)):
             t = t + rp.Dt
-            rows.append(_row(model, t, sums[k], n_traj))
+            rows.append(_row(model, t, sums[k], n_traj, _linear))
     else:
         T, Dt = rp.T, rp.Dt
         t = front_time()
@@ -84,13 +87,13 @@ def evolve(script, args=(), rng=None, precision=None, n_traj=None, resume=None):
             if n:
                 sums = ens.run(Dt, n)
                 for k in range(n):
-                    rows.append(_row(model, ts[k], sums[k], n_traj))
+                    rows.append(_row(model, ts[k], sums[k], n_traj, _linear))
                 t = ts[-1]
             else:
                 delta = T - t
                 sums = ens.run(delta, 1)
                 t = t + delta
-                rows.append(_row(model, t, sums[0], n_traj))
+                rows.append(_row(model, t, sums[0], n_traj, _linear))
     return np.array(rows), ens, model
 
 
@@ -199,3 +202,21 @@ def _evolve_master(model, rp):
             t = t + delta
             rows.append(row(t, vals))
     return np.array(rows), m, model
+
+
+def time_averaged(script, args=(), relaxation_time=0.0, **kw):
+    """quantumtrajectory::TimeAveragingMCWF_Trajectory (TimeAveragingMCWF_Trajectory.h:35-90):
+    the run of ``evolve`` with, at every stream after the relaxation time, the running mean
+    of the unprocessed averages, averages = (averages * n + now) / (n + 1), without step-size
+    weighting.  Returns (rows, processed time averages or None, number of samples, ensemble,
+    model); the reference prints the processed averages in its end-of-run log ("Time
+    averages after relaxation time ...")."""
+    linear = []
+    rows, ens, model = evolve(script, args, _linear=linear, **kw)
+    acc = np.zeros(model.n_avr)
+    n = 0
+    for t, now in zip(rows[:, 0], linear):
+        if t > relaxation_time:
+            acc = (acc * n + now) / (n + 1)
+            n += 1
+    return rows, (model.process(acc.copy()) if n else None), n, ens, model

@@ -627,3 +627,16 @@ def test_finite_temperature_mode_ensemble_vs_master(gpu, oracle):
     model = gpu.Model("PumpedLossyMode_C++QED", C1_ARGS + ["--nTh", "0.5"])
     z = _ensemble_vs_master_z(gpu, oracle, model, 4096, 0.25, 6, [0, 2, 3])
     assert z.max() < 4.0, z
+
+
+def test_time_averaged_trajectory_reaches_the_coherent_steady_state(gpu):
+    """TimeAveragingMCWF_Trajectory: one trajectory of the driven lossy mode (Delta = -1,
+    eta = 2, kappa = 1) stays a coherent state (jumps do not change it), so its time average
+    after relaxation is the analytic steady state alpha = eta / (kappa - i Delta) = 1 - i:
+    <n> = VAR(n) = 2, Re<a> = 1, Im<a> = -1."""
+    from cppqed_b200.evolve import time_averaged
+
+    args = C1_ARGS + ["--evol", "single", "--T", "40", "--Dt", "0.5", "--dc", "0"]
+    rows, avg, n, _, _ = time_averaged("PumpedLossyMode_C++QED", args, relaxation_time=15.0)
+    assert n == int(np.sum(rows[:, 0] > 15.0)) and n > 40
+    assert np.allclose(avg, [2.0, 2.0, 1.0, -1.0], atol=2e-3), avg
