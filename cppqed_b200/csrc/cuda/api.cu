@@ -465,8 +465,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       ck(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming), "cudaEventCreate");
     }
     g.threads = pars->cta_threads > 0 ? pars->cta_threads : defaultThreads(g);
-    if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 256 : 128))
-      return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 256");
+    if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 512 : 128))
+      return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 512");
     g.smemVectors = pars->cta_threads > 0 && pars->cta_shared_vectors && sharedVectorsFit(g, e->elemBytes, e->device);
   }
   if (pars->autotune && pars->cta_threads <= 0)
@@ -631,7 +631,7 @@ std::vector<int> threadCandidates(const KernelGroup& g, bool vectorsFit) {
   std::vector<int> c;
   if (g.kind == 0) return {64, 128};
   for (int q = 1; q <= 4; ++q) {  // rows per thread
-    const int t = std::min(256, std::max(64, ((g.Dmax + q - 1) / q + 31) / 32 * 32));
+    const int t = std::min(512, std::max(64, ((g.Dmax + q - 1) / q + 31) / 32 * 32));
     if (std::find(c.begin(), c.end(), t) == c.end()) c.push_back(t);
   }
   if (std::find(c.begin(), c.end(), 256) == c.end()) c.push_back(256);

@@ -468,7 +468,7 @@ struct BlockWorker {
 // Dynamic shared memory: two stage buffers of `smemD` elements, the reduction scratch,
 // then 8 broadcast words.
 template <typename R, bool IP>
-__global__ void __launch_bounds__(256) mcwfBlockKernel(TrajDev td, RunArgs ra, BlockScratch bsc, int smemD) {
+__global__ void __launch_bounds__(512, 1) mcwfBlockKernel(TrajDev td, RunArgs ra, BlockScratch bsc, int smemD) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char blockSmem[];
   C2* ys0 = reinterpret_cast<C2*>(blockSmem);

@@ -502,7 +502,7 @@ int cqg_server_create(const cqg_server_pars* p, cqg_server** out) {
       g.kind = key == kMaxGroups ? 1 : 0;
       g.E = g.kind ? 0 : key;
       g.threads = m.cta_threads > 0 ? m.cta_threads : defaultThreads(g);
-      if (g.threads % 32 || g.threads > (g.kind ? 256 : 128))
+      if (g.threads % 32 || g.threads > (g.kind ? 512 : 128))
         return fail(CQG_E_INVALID, "cqg_server_create: cta_threads must be a multiple of 32, at most 128");
       ck(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "cudaStreamCreate");
       ck(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming), "cudaEventCreate");

@@ -138,7 +138,9 @@ typedef struct cqg_mcwf_pars {
   int32_t autotune;            /* 1: time the candidate CTA shapes of each kernel group on a
                                   sample of its trajectories at creation and keep the fastest
                                   (cached per shape class and device); 0: fixed defaults */
-  int32_t cta_threads;         /* > 0: force this CTA size on every group (no tuning) */
+  int32_t cta_threads;         /* > 0: force this CTA size on every group (no tuning); a
+                                  multiple of 32, at most 128 for warp-per-trajectory groups
+                                  and 512 for CTA-per-trajectory groups */
   int32_t cta_shared_vectors;  /* with cta_threads > 0, for CTA-per-trajectory groups: 1 keeps
                                   the stage derivatives in shared memory (when they fit), 0 in
                                   a global scratch slab; the autotuner chooses otherwise */

@@ -412,7 +412,7 @@ def test_cta_shape_does_not_change_warp_trajectories(gpu):
 
 
 def test_block_kernel_cta_shapes_agree(gpu):
-    """The CTA-per-trajectory kernel with 64, 160 and 256 threads (one to three rows per
+    """The CTA-per-trajectory kernel with 64, 160, 256 and 512 threads (one to eight rows per
     thread at D = 450) follows the same trajectories up to the summation order."""
     model = gpu.Model("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30",
                                         "--etaOpt", "2", "--kappaOpt", "1", "--deltaCOpt", "-1",
@@ -420,7 +420,7 @@ def test_block_kernel_cta_shapes_agree(gpu):
     sysd = gpu.System(model.desc)
     n = 6
     runs = []
-    for cta in (256, 160, 64):
+    for cta in (256, 512, 160, 64):
         pars = model.run_pars().mcwf
         pars.cta_threads = cta
         ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
