@@ -55,6 +55,9 @@ class cqg_observable(C.Structure):
         ("dense_axis", C.c_int32),
         ("col_re", C.c_int32),
         ("col_im", C.c_int32),
+        ("fourier", C.c_int32),
+        ("reserved", C.c_int32),
+        ("fourier_weights", C.POINTER(C.c_double)),
     ]
 
 

@@ -150,7 +150,8 @@ void buildSystemDevice(cqg_system& s) {
   std::vector<int> jcol(size_t(nJ) * SJ * D), ocol(size_t(nObs) * SO * D);
   std::vector<dcomp> jval(size_t(nJ) * SJ * D), oval(size_t(nObs) * SO * D);
   std::vector<double> jw(size_t(nJ) * D, 0.);
-  std::vector<int> jHasW(nJ), oRe(nObs), oIm(nObs), oS(nObs);
+  std::vector<int> jHasW(nJ), oRe(nObs), oIm(nObs), oS(nObs), oF(nObs, 0);
+  for (int k : L.fourierObs) oF[k] = 1;
   for (int m = 0; m < nJ; ++m) {
     const auto& J = L.jumps[m];
     for (int k = 0; k < SJ; ++k)
@@ -179,6 +180,7 @@ void buildSystemDevice(cqg_system& s) {
   const size_t oCol = A.add(H.col.size() * 4 + 4), oJcol = A.add(jcol.size() * 4 + 4), oJw = A.add(jw.size() * 8 + 8),
                oJHasW = A.add(jHasW.size() * 4 + 4), oOcol = A.add(ocol.size() * 4 + 4),
                oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4), oOS = A.add(oS.size() * 4 + 4),
+               oOF = A.add(oF.size() * 4 + 4), oFW = A.add(L.fourierW.size() * 8 + 8),
                oFreq = A.add(H.freq.size() * 16 + 16), oLambda = A.add(L.lambda.size() * 16 + 16),
                oDiagD = A.add(H.diag.size() * 16 + 16), oValD = A.add(H.val.size() * 16 + 16),
                oJvalD = A.add(jval.size() * 16 + 16), oDiagF = A.add(H.diag.size() * 8 + 8),
@@ -194,6 +196,8 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oORe, oRe);
   upload(b, oOIm, oIm);
   upload(b, oOS, oS);
+  upload(b, oOF, oF);
+  upload(b, oFW, L.fourierW);
   upload(b, oFreq, toD2(H.freq));
   upload(b, oLambda, toD2(L.lambda));
   upload(b, oDiagD, toD2(H.diag));
@@ -222,6 +226,14 @@ void buildSystemDevice(cqg_system& s) {
   sd.oRe = reinterpret_cast<const int*>(b + oORe);
   sd.oIm = reinterpret_cast<const int*>(b + oOIm);
   sd.oS = reinterpret_cast<const int*>(b + oOS);
+  sd.oFourier = reinterpret_cast<const int*>(b + oOF);
+  sd.fW = reinterpret_cast<const double*>(b + oFW);
+  sd.nF = int(L.fourierObs.size());
+  sd.fN = int(L.fourierN);
+  sd.fStride = int(L.fourierStride);
+  sd.fLog2 = 0;
+  while ((int64_t(1) << sd.fLog2) < L.fourierN) ++sd.fLog2;
+  for (int k = 0; k < 4; ++k) sd.fObs[k] = k < sd.nF ? L.fourierObs[size_t(k)] : -1;
   sd.freq = H.freq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFreq);
   sd.lambda = L.lambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oLambda);
   sd.diagD = reinterpret_cast<const double2*>(b + oDiagD);

@@ -93,7 +93,6 @@ struct BlockWorker {
   __device__ __forceinline__ C2* xnew() const { return vec + 6 * stride; }
   __device__ __forceinline__ C2* cache() const { return vec + 7 * stride; }
 
-  // out = (H/i) y, y in shared memory
   // out = (H/i) y at picture time tau, y in shared memory
   __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
     ++nRhs;
@@ -370,12 +369,58 @@ struct BlockWorker {
     return true;
   }
 
+  // Observables sum_slices sum_x w_k[x] |(F psi_slice)_x|^2 with F the k -> x transform of
+  // quantumdata::ffTransform (LazyDensityOperatorFFT.cc:12-31): radix-2 backward DFT of each
+  // slice along the axis (one warp per slice, in the second stage buffer), then
+  // (F psi)_x = (-1)^x y_{(x + N/2) mod N} / sqrt(N), whose sign does not enter |.|^2.
+  // The state is staged in ys0 by the caller.
+  __device__ __noinline__ void fourierAverages(double* out) {
+    const int N = sysp->fN, logN = sysp->fLog2, stride = sysp->fStride, nF = sysp->nF;
+    const int nSlices = D / N, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double v[4] = {0., 0., 0., 0.};
+    if (warp < nSlices) {
+      C2* buf = ys1 + size_t(warp) * N;  // nSlices * N = D elements, one slice per warp
+      for (int j = warp; j < nSlices; j += nw) {
+        const int base = (j / stride) * (N * stride) + (j % stride);
+        for (int m = lane; m < N; m += 32) buf[__brev(unsigned(m)) >> (32 - logN)] = ys0[base + m * stride];
+        __syncwarp();
+        for (int len = 2; len <= N; len <<= 1) {
+          const int half = len >> 1;
+          for (int bf = lane; bf < (N >> 1); bf += 32) {
+            const int pos = bf % half, i0 = (bf / half) * len + pos, i1 = i0 + half;
+            double sw, cw;
+            sincospi(double(2 * pos) / double(len), &sw, &cw);  // exp(+2 pi i pos / len)
+            const C2 a = buf[i0], bb = buf[i1];
+            const R tx = R(cw) * bb.x - R(sw) * bb.y, ty = R(cw) * bb.y + R(sw) * bb.x;
+            buf[i0] = mk<C2>(double(a.x + tx), double(a.y + ty));
+            buf[i1] = mk<C2>(double(a.x - tx), double(a.y - ty));
+          }
+          __syncwarp();
+        }
+        for (int m = lane; m < N; m += 32) {
+          const C2 yv = buf[(m + (N >> 1)) & (N - 1)];
+          const double p = (double(yv.x) * double(yv.x) + double(yv.y) * double(yv.y)) / double(N);
+          for (int f = 0; f < nF; ++f) v[f] += __ldg(&sysp->fW[size_t(f) * N + m]) * p;
+        }
+        __syncwarp();
+      }
+    }
+    blockSumN(v, nF, red);
+    if (threadIdx.x == 0 && out)
+      for (int f = 0; f < nF; ++f) {
+        const int k = sysp->fObs[f];
+        if (sysp->oRe[k] >= 0) out[sysp->oRe[k]] = v[f];
+      }
+  }
+
   __device__ __forceinline__ void averages(double* out) {
     __syncthreads();
     for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
     __syncthreads();
-    const int nObs = sysp->nObs, SO = sysp->SO;
+    const int nObs = sysp->nObs, SO = sysp->SO, nF = sysp->nF;
+    if (nF) fourierAverages(out);
     for (int k = 0; k < nObs; ++k) {
+      if (nF && sysp->oFourier[k]) continue;
       const double2* ov = sysp->oval + size_t(k) * SO * D;
       const int* oc = sysp->ocol + size_t(k) * SO * D;
       const int nSk = sysp->oS[k];

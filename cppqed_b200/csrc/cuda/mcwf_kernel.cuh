@@ -157,6 +157,12 @@ struct SysDev {
   const int* oRe;        // [nObs]
   const int* oIm;        // [nObs]
   const int* oS;         // [nObs] slots used by each observable (<= SO; the rest is padding)
+  // observables that the CTA kernel evaluates with a fast k -> x transform along one axis
+  int nF;                // how many (0: none)
+  int fN, fLog2, fStride;
+  int fObs[4];           // their observable indices
+  const int* oFourier;   // [nObs] 1: evaluated by the transform (CTA kernel), else 0
+  const double* fW;      // [nF][fN] weights
   const double2* freq;   // [S][D] (IP) or null
   const double2* lambda; // [D] (Exact) or null
   // precision-specific copies

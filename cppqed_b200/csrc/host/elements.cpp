@@ -691,6 +691,12 @@ void fillParticleAveraged(Element& e, const Spatial& space) {
   x.colRe = 2;
   x2.dense = dense(2);
   x2.colRe = 3;
+  x.fourierWeights.resize(N);
+  x2.fourierWeights.resize(N);
+  for (size_t m = 0; m < N; ++m) {
+    x.fourierWeights[m] = space.x(m);
+    x2.fourierWeights[m] = space.x(m) * space.x(m);
+  }
   e.obs = {p, p2, x, x2};
   e.process = [](double* avr) {
     avr[1] -= avr[0] * avr[0];

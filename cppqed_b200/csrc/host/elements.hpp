@@ -39,6 +39,7 @@ struct ElementObservable {
   CVec dense;      // dense N x N on `denseAxis`
   int denseAxis = 0;
   int colRe = -1, colIm = -1;  // local average columns
+  DVec fourierWeights;  // non-empty: dense = F^+ diag(w) F with F the k -> x transform
 };
 
 struct Element;

@@ -222,6 +222,34 @@ LoweredSystem lowerSystem(const cqg_system_desc& d) {
     L.obsColRe.push_back(o.col_re);
     L.obsColIm.push_back(o.col_im);
   }
+  // fast-transform candidates
+  int fAxis = -1;
+  bool fOk = true;
+  for (int k = 0; k < d.n_obs; ++k) {
+    const auto& o = d.obs[k];
+    if (!o.fourier) continue;
+    if (!o.dense || !o.fourier_weights || o.col_im >= 0 || (fAxis >= 0 && o.dense_axis != fAxis)) {
+      fOk = false;
+      continue;
+    }
+    fAxis = o.dense_axis;
+    L.fourierObs.push_back(k);
+  }
+  if (fAxis >= 0) {
+    const int64_t N = s.dims[fAxis];
+    if (!fOk || N < 2 || N > 2048 || (N & (N - 1)) || L.fourierObs.size() > 4) {
+      L.fourierObs.clear();
+    } else {
+      L.fourierN = N;
+      L.fourierStride = s.strides[fAxis];
+      for (int k : L.fourierObs)
+        for (int64_t m = 0; m < N; ++m) {
+          const double w = d.obs[k].fourier_weights[m];
+          if (!std::isfinite(w)) throw std::invalid_argument("obs: non-finite fourier weight");
+          L.fourierW.push_back(w);
+        }
+    }
+  }
   return L;
 }
 

@@ -38,6 +38,12 @@ struct LoweredSystem {
   std::vector<std::vector<double>> weights;  // [m][D] closed-form rate weights (empty: ||J psi||^2)
   std::vector<EllOperator> obs;        // observables, slots include diagonal entries
   std::vector<int> obsColRe, obsColIm;
+  // Observables that may be evaluated by a fast k -> x transform along one axis (all on the
+  // same axis, N = 2^n <= 2048 points, real-valued): their indices, the axis' length and
+  // stride, and their weights [nFourier][N].  Empty when none or when the conditions fail.
+  std::vector<int> fourierObs;
+  int64_t fourierN = 0, fourierStride = 0;
+  std::vector<double> fourierW;
   int nAvr = 0;
   double highestFrequency = 0;
 };

@@ -144,6 +144,11 @@ void System::lower() {
         co.dense = store(o.dense);
         co.dense_axis = p.axes.at(o.denseAxis);
         co.op.rank = 0;
+        if (!o.fourierWeights.empty()) {
+          weights_.push_back(o.fourierWeights);
+          co.fourier = 1;
+          co.fourier_weights = weights_.back().data();
+        }
       } else {
         co.op = place(o.op, p.axes);
       }

@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 #define CQG_MAX_RANK 8
-#define CQG_ABI_VERSION 3
+#define CQG_ABI_VERSION 4
 
 /* ---- status codes ------------------------------------------------------ */
 #define CQG_OK 0
@@ -93,6 +93,15 @@ typedef struct cqg_observable {
   int32_t dense_axis;
   int32_t col_re; /* output column of Re<O>, or -1 */
   int32_t col_im; /* output column of Im<O>, or -1 */
+  /* fourier != 0 (with a dense matrix on dense_axis that is this same operator): the
+   * observable is also given as the sum over the 1-D slices along dense_axis of
+   * sum_x fourier_weights[x] |(F psi_slice)_x|^2, F the reference's k -> x transform
+   * (quantumdata::ffTransform, LazyDensityOperatorFFT.cc:12-31), e.g. a particle's <X> and
+   * <X^2> (Particle.cc:128-160).  The engine may then use a fast transform instead of the
+   * dense matrix; the value is real (col_im must be -1). */
+  int32_t fourier;
+  int32_t reserved;
+  const double* fourier_weights; /* [dims[dense_axis]] */
 } cqg_observable;
 
 /* The whole system: Hamiltonian terms H/i in the reference's application

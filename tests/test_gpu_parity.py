@@ -640,3 +640,32 @@ def test_time_averaged_trajectory_reaches_the_coherent_steady_state(gpu):
     rows, avg, n, _, _ = time_averaged("PumpedLossyMode_C++QED", args, relaxation_time=15.0)
     assert n == int(np.sum(rows[:, 0] > 15.0)) and n > 40
     assert np.allclose(avg, [2.0, 2.0, 1.0, -1.0], atol=2e-3), avg
+
+
+def test_particle_position_averages_by_fast_transform_match_dense(gpu):
+    """The CTA kernel evaluates the particle's <X> and <X^2> with a radix-2 transform of each
+    slice; the allocation-free averages entry point evaluates the same observables as dense
+    matrices F^+ diag(x) F.  Both give the same ensemble sums on the same states."""
+    import ctypes
+
+    import torch
+
+    model = gpu.Model("1particle1mode", PARTICLE_ARGS)
+    sysd = gpu.System(model.desc)
+    n = 64
+    pars = model.run_pars().mcwf
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    assert ens.plan()[0]["kind"] in (1, 2)
+    ens.run(0.1, 2)
+    fast = ens.steps(0, 1.0)[:model.n_avr]
+    psi = np.stack([ens.state(i, model.dim) for i in range(n)])
+    d_psi = torch.from_numpy(psi).to("cuda")
+    d_sums = torch.zeros(model.n_avr, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    rc = gpu.lib().cqg_system_averages_noalloc(sysd._h, ctypes.c_void_p(d_psi.data_ptr()), n,
+                                               ctypes.c_void_p(d_sums.data_ptr()), None)
+    assert rc == A.CQG_OK, gpu.lib().cqg_last_error()
+    torch.cuda.synchronize()
+    dense = d_sums.cpu().numpy()
+    assert np.allclose(fast, dense, rtol=1e-11, atol=1e-12), (fast, dense)
+    assert abs(dense[6]) > 1e-3 and dense[7] > 1e-3  # <X> and <X^2> columns are not trivially zero
