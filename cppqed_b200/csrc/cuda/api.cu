@@ -23,6 +23,38 @@ using namespace cqg::engine;
 
 namespace {
 
+// A process-wide pinned host buffer for staging uploads (grown on demand, kept until exit,
+// one user at a time).
+class HostStaging {
+ public:
+  explicit HostStaging(size_t bytes) : lock_(mutex()) {
+    Buf& b = buf();
+    if (b.size < bytes) {
+      if (b.ptr) cudaFreeHost(b.ptr);
+      b.ptr = nullptr;
+      b.size = 0;
+      ck(cudaHostAlloc(&b.ptr, bytes, cudaHostAllocPortable), "cudaHostAlloc(staging)");
+      b.size = bytes;
+    }
+  }
+  char* data() { return static_cast<char*>(buf().ptr); }
+
+ private:
+  struct Buf {
+    void* ptr = nullptr;
+    size_t size = 0;
+  };
+  static std::mutex& mutex() {
+    static std::mutex m;
+    return m;
+  }
+  static Buf& buf() {
+    static Buf b;
+    return b;
+  }
+  std::lock_guard<std::mutex> lock_;
+};
+
 // single device allocation carved into aligned sub-buffers
 struct Arena {
   std::vector<std::pair<size_t, size_t>> parts;  // offset, size
@@ -370,51 +402,64 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
                oJT = A.add(nTraj * e->jumpCap * 8), oJL = A.add(nTraj * e->jumpCap * 4), oJN = A.add(nTraj * 8),
                oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(kMaxGroups * sizeof(int)), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
   ck(cudaMalloc(&e->dmem, A.total), "cudaMalloc(ensemble)");
-  ck(cudaMemset(e->dmem, 0, A.total), "cudaMemset");
   char* b = static_cast<char*>(e->dmem);
 
-  // host-side initial values
-  std::vector<double> t(nTraj, 0.), t0(nTraj, 0.), dtTry(nTraj), dtDid(nTraj, 0.);
-  std::vector<unsigned long long> rng(4 * nTraj, 0), cnt(8 * nTraj, 0);
-  std::vector<unsigned char> psiBytes(size_t(psiElems) * e->elemBytes);
+  // Host image of the arena's first part (states, offsets, indices, times, random streams,
+  // counters) in a pinned staging buffer, sent in one copy; the rest is zeroed on the device.
+  {  // the staging buffer is held only for this block (the autotuner below creates ensembles)
+  HostStaging staging(oMax);
+  char* h = staging.data();
+  const long long* offs = e->psiOff.data();
+  std::memcpy(h + oOff, offs, size_t(nTraj) * 8);
+  std::memcpy(h + oIdx, e->sysIdx.data(), size_t(nTraj) * 4);
+  auto* ht = reinterpret_cast<double*>(h + oT);
+  auto* ht0 = reinterpret_cast<double*>(h + oT0);
+  auto* hTry = reinterpret_cast<double*>(h + oTry);
+  auto* hDid = reinterpret_cast<double*>(h + oDid);
+  auto* hRng = reinterpret_cast<unsigned long long*>(h + oRng);
+  auto* hCnt = reinterpret_cast<unsigned long long*>(h + oCnt);
+  std::memset(hRng, 0, size_t(nTraj) * 32);
+  std::memset(hCnt, 0, size_t(nTraj) * 64);
   double dt0Shared = 0.;
   bool overshotShared = false;
+  std::vector<dcomp> psi;
+  std::vector<unsigned char> one;  // the converted state of the current initial state
   for (int64_t i = 0; i < nTraj; ++i) {
     const cqg_system* s = systems[e->sysIdx[i]];
     const int64_t D = s->L.D;
-    const cqg_complex* p = psi0s + (psi0Off ? psi0Off[i] : 0);
-    std::vector<dcomp> psi(D);
-    for (int64_t k = 0; k < D; ++k) psi[k] = dcomp(p[k].re, p[k].im);
-    for (int64_t k = 0; k < D; ++k) {
-      if (e->elemBytes == 16) {
-        double2 v = make_double2(psi[k].real(), psi[k].imag());
-        std::memcpy(&psiBytes[(e->psiOff[i] + k) * 16], &v, 16);
-      } else {
-        float2 v = make_float2(float(psi[k].real()), float(psi[k].imag()));
-        std::memcpy(&psiBytes[(e->psiOff[i] + k) * 8], &v, 8);
+    if (psi0Off || i == 0) {  // one initial state for a whole ensemble: convert it once
+      const cqg_complex* p = psi0s + (psi0Off ? psi0Off[i] : 0);
+      psi.resize(D);
+      for (int64_t k = 0; k < D; ++k) psi[k] = dcomp(p[k].re, p[k].im);
+      one.resize(size_t(D) * e->elemBytes);
+      for (int64_t k = 0; k < D; ++k) {
+        if (e->elemBytes == 16) {
+          const double2 v = make_double2(psi[k].real(), psi[k].imag());
+          std::memcpy(&one[k * 16], &v, 16);
+        } else {
+          const float2 v = make_float2(float(psi[k].real()), float(psi[k].imag()));
+          std::memcpy(&one[k * 8], &v, 8);
+        }
       }
+      dt0Shared = initialDtTry(*s, psi, *pars, &overshotShared);
     }
+    std::memcpy(h + oPsi + size_t(offs[i]) * e->elemBytes, one.data(), one.size());
     if (pars->rng == CQG_RNG_PCG64) {
       const auto g = dev::Pcg64::seeded(pars->seed, pars->prng_stream + uint64_t(i));
-      rng[4 * i + 0] = g.state.hi;
-      rng[4 * i + 1] = g.state.lo;
-      rng[4 * i + 2] = g.inc.hi;
-      rng[4 * i + 3] = g.inc.lo;
+      hRng[4 * i + 0] = g.state.hi;
+      hRng[4 * i + 1] = g.state.lo;
+      hRng[4 * i + 2] = g.inc.hi;
+      hRng[4 * i + 3] = g.inc.lo;
     }
-    // one initial state for the whole ensemble: its initial step once
-    if (psi0Off || i == 0) dt0Shared = initialDtTry(*s, psi, *pars, &overshotShared);
-    if (overshotShared) cnt[8 * i + 4] += 1;
-    dtTry[i] = dt0Shared;
+    if (overshotShared) hCnt[8 * i + 4] = 1;
+    ht[i] = 0.;
+    ht0[i] = 0.;
+    hTry[i] = dt0Shared;
+    hDid[i] = 0.;
   }
-  ck(cudaMemcpy(b + oPsi, psiBytes.data(), psiBytes.size(), cudaMemcpyHostToDevice), "cudaMemcpy(psi)");
-  upload(b, oOff, e->psiOff);
-  upload(b, oIdx, e->sysIdx);
-  upload(b, oT, t);
-  upload(b, oT0, t0);
-  upload(b, oTry, dtTry);
-  upload(b, oDid, dtDid);
-  upload(b, oRng, rng);
-  upload(b, oCnt, cnt);
+  ck(cudaMemcpy(b, h, oMax, cudaMemcpyHostToDevice), "cudaMemcpy(ensemble)");
+  }
+  ck(cudaMemset(b + oMax, 0, A.total - oMax), "cudaMemset");
   std::vector<dev::SysDev> sds;
   for (auto* s : e->systems) sds.push_back(s->sd);
   upload(b, oSys, sds);
