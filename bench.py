@@ -320,8 +320,9 @@ def run_ours(args, rank, world, dev):
     clocks = sampler.stop() if rank == 0 else None
     c1 = ens.counters()
     d = (c1.astype(np.int64) - c0.astype(np.int64)).sum(axis=0)
-    steps_local, attempts_local, rhs_local = int(d[0]), int(d[1]), int(d[3])
-    tot = allreduce(np.array([steps_local, attempts_local, rhs_local], dtype=np.float64))
+    # summed over ranks: accepted steps, ODE attempts, RHS evaluations, failed attempts,
+    # dpLimit overshoots, step-backs, jumps
+    tot = allreduce(np.array([d[0], d[1], d[3], d[2], d[4], d[5], d[6]], dtype=np.float64))
     tmax = sharding.max_over_ranks([run_ms, kernel_ms], world)
     run_ms_max, kernel_ms_max = float(tmax[0]), float(tmax[1])
     steps_total = float(tot[0])
@@ -360,6 +361,8 @@ def run_ours(args, rank, world, dev):
     return {
         "value": value, "ms_per_step": run_ms_max / args.steps, "steps_total": steps_total,
         "attempts_total": float(tot[1]), "rhs_total": float(tot[2]), "kernel_ms": kernel_ms_max,
+        "failed_total": float(tot[3]), "overshoots_total": float(tot[4]), "stepbacks_total": float(tot[5]),
+        "jumps_total": float(tot[6]),
         "clocks": clocks, "e2e": {"value": e2e_value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": h2d,
                                   "d2h_bytes_per_step": d2h, "steps_per_call": e2e_steps / n_e2e,
                                   "ms_per_call": dict(zip(("create", "run", "counters", "destroy"),
@@ -672,7 +675,9 @@ def main():
                "clocks": r["clocks"],
                "gpu_launches": 3 * args.steps,
                "counters": {"accepted_steps": r["steps_total"], "ode_attempts": r["attempts_total"],
-                            "rhs_evaluations": r["rhs_total"], "kernel_ms": r["kernel_ms"]}}
+                            "rhs_evaluations": r["rhs_total"], "failed_attempts": r["failed_total"],
+                            "dp_limit_overshoots": r["overshoots_total"], "step_backs": r["stepbacks_total"],
+                            "jumps": r["jumps_total"], "kernel_ms": r["kernel_ms"]}}
         print(json.dumps(out))
     if world > 1:
         torch.distributed.barrier()

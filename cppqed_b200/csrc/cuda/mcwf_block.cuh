@@ -144,16 +144,15 @@ struct BlockWorker {
       const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
               e5 = R(dt * CK::e5);
       const double adt = fabs(dt);
-      double errLocal = 0.;
+      ErrNormMax errLocal;
       for (int r = threadIdx.x; r < D; r += blockDim.x) {
         const C2 xr = x[r], k0 = K(0)[r], k2 = K(2)[r], k3 = K(3)[r], k4 = K(4)[r], k5 = K(5)[r];
         xnew()[r] = axpy(b5, k5, axpy(b3, k3, axpy(b2, k2, axpy(b0, k0, xr))));
         C2 xe = mk<C2>(0, 0);
         xe = axpy(e5, k5, axpy(e4, k4, axpy(e3, k3, axpy(e2, k2, axpy(e0, k0, xe)))));
-        const double den = ra.absSlot + ra.relSlot * (cabs(xr) + adt * cabs(k0));
-        errLocal = fmax(errLocal, cabs(xe) / den);
+        errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(xr) + adt * cabs(k0)));
       }
-      const double err = blockMax(errLocal, red);
+      const double err = blockMax(errLocal.value(), red);
       if (!(err == err)) {
         status |= 1u;
         return false;
