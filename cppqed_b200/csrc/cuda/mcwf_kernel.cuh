@@ -312,6 +312,10 @@ struct Worker {
   C2 diag[E];
   C2 cval[CREG ? SMAX : 1][E];
   int ccol[CREG ? SMAX : 1][E];
+  // Otherwise the column indices still live in registers, one byte per slot (a warp's rows
+  // are < 128), so that the gather from the staged state does not wait for a table load.
+  static constexpr int CPACK = CREG ? 1 : (SMAX + 3) / 4;
+  unsigned cpack[CPACK][E];
 
   // trajectory state
   C2 x[E];
@@ -356,6 +360,17 @@ struct Worker {
           ccol[s][e] = vs ? col[s * D + r] : 0;
           cval[s][e] = vs ? val[s * D + r] : mk<C2>(0, 0);
         }
+      } else {
+#pragma unroll
+        for (int w = 0; w < CPACK; ++w) {
+          unsigned p = 0u;
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int s = 4 * w + b;
+            if (s < SMAX && v && s < S) p |= unsigned(col[s * D + r]) << (8 * b);
+          }
+          cpack[w][e] = p;
+        }
       }
     }
   }
@@ -398,7 +413,7 @@ struct Worker {
             cc = ccol[s][e];
           } else {
             c = valid(e) ? __ldg(&val[s * D + r]) : mk<C2>(0, 0);
-            cc = __ldg(&col[s * D + r]);
+            cc = int((cpack[s >> 2][e] >> (8 * (s & 3))) & 0xffu);
           }
           if (IP && hasFreq && valid(e)) {
             if (phsOn) {
