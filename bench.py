@@ -33,6 +33,11 @@ WORKLOADS = {
     "qbitmode_jc_2x40": ("QbitMode_C++QED",
                          ["--picture", "Sch", "--deltaA", "0", "--gamma", "0.5", "--deltaC", "0", "--kappa", "1",
                           "--eta", "1.5", "--cutoff", "40", "--g", "2"], 4096, 1.0),
+    # the same system in the interaction picture (the reference's default picture): detuned
+    # qubit and mode, so the coupling and pump terms carry time-dependent phases
+    "qbitmode_jc_2x40_ip": ("QbitMode_C++QED",
+                            ["--picture", "IP", "--deltaA", "-1", "--gamma", "0.5", "--deltaC", "2", "--kappa", "1",
+                             "--eta", "1.5", "--cutoff", "40", "--g", "2"], 4096, 1.0),
     # particle in a cavity (1particle1mode, ParticleAlongCavity with a cos^2 mode function,
     # no transverse pump): mode cutoff 20 x particle momenta 2^7 = 2560
     "particle_cavity_2560": ("1particle1mode",

@@ -94,7 +94,7 @@ class cqg_mcwf_pars(C.Structure):
         ("autotune", C.c_int32),
         ("cta_threads", C.c_int32),
         ("cta_shared_vectors", C.c_int32),
-        ("reserved", C.c_int32),
+        ("ip_phase_table", C.c_int32),
     ]
 
 

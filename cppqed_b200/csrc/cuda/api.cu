@@ -81,8 +81,9 @@ struct cqg_ensemble {
   std::vector<long long> psiOff;
   std::vector<KernelGroup> groups;
   size_t elemBytes = 16;
-  // device buffers
+  // device buffers (recycled blocks: deviceAlloc / deviceRelease)
   void* dmem = nullptr;
+  size_t dmemBytes = 0;
   dev::TrajDev td{};
   dev::SysDev* dSystems = nullptr;
   int* dQueue = nullptr;  // one work-queue counter per group
@@ -94,25 +95,112 @@ struct cqg_ensemble {
   size_t sumsCap = 0;
   int jumpCap = 64;
   ~cqg_ensemble() {
+    // nothing of this ensemble may still run on the blocks that go back to the cache
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    for (auto& g : groups)
+      if (g.stream) cudaStreamSynchronize(g.stream);
+    if (stream) cudaStreamSynchronize(stream);
     for (auto& g : groups) {
-      if (g.scratch) cudaFree(g.scratch);
+      cqg::engine::deviceRelease(device, g.scratch, g.scratchBytes);
       if (g.done) cudaEventDestroy(g.done);
       if (g.stream) cudaStreamDestroy(g.stream);
     }
-    if (dAvr) cudaFree(dAvr);
-    if (dSums) cudaFree(dSums);
-    if (dmem) cudaFree(dmem);
+    cqg::engine::deviceRelease(device, dAvr, avrCap * sizeof(double));
+    cqg::engine::deviceRelease(device, dSums, sumsCap * sizeof(double));
+    cqg::engine::deviceRelease(device, dmem, dmemBytes);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evRun0) cudaEventDestroy(evRun0);
     if (evRun1) cudaEventDestroy(evRun1);
     if (evFork) cudaEventDestroy(evFork);
     if (stream) cudaStreamDestroy(stream);
+    cudaSetDevice(cur);
   }
 };
 
 namespace cqg {
 namespace engine {
+
+// ---- recycled device blocks -----------------------------------------------------------
+// Ensembles are created and destroyed at a high rate by services, parameter sweeps and
+// benchmarks, and cudaMalloc / cudaFree cost driver work (cudaFree also synchronises the
+// device).  Freed ensemble buffers are kept per (device, size class) and handed to the
+// next request of that class: sizes round up to a power of two from 4 KiB to 2 MiB and to a
+// multiple of 2 MiB above.  At most kCacheCap bytes stay cached per device; a cudaMalloc
+// that fails returns the device's cached blocks to the driver and is retried once.
+namespace blockcache {
+constexpr size_t kCacheCap = size_t(8) << 30;
+struct BlockCache {
+  std::mutex mu;
+  std::map<std::pair<int, size_t>, std::vector<void*>> blocks;
+  std::map<int, size_t> cached;
+};
+BlockCache& blockCache() {
+  static BlockCache* c = new BlockCache;  // never destroyed: blocks outlive static teardown
+  return *c;
+}
+size_t sizeClass(size_t b) {
+  const size_t grain = size_t(2) << 20;
+  if (b >= grain) return (b + grain - 1) / grain * grain;
+  size_t c = 4096;
+  while (c < b) c <<= 1;
+  return c;
+}
+void trimDevice(BlockCache& c, int device) {  // caller holds c.mu and has device current
+  for (auto it = c.blocks.begin(); it != c.blocks.end();) {
+    if (it->first.first == device) {
+      for (void* p : it->second) cudaFree(p);
+      it = c.blocks.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  c.cached[device] = 0;
+}
+}  // namespace blockcache
+
+void* deviceAlloc(size_t bytes, const char* what) {
+  using namespace blockcache;
+  int device = 0;
+  ck(cudaGetDevice(&device), "cudaGetDevice");
+  const size_t sz = sizeClass(bytes);
+  BlockCache& c = blockCache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  auto it = c.blocks.find({device, sz});
+  if (it != c.blocks.end() && !it->second.empty()) {
+    void* p = it->second.back();
+    it->second.pop_back();
+    c.cached[device] -= sz;
+    return p;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, sz) != cudaSuccess) {
+    cudaGetLastError();  // clear the allocation error before retrying
+    trimDevice(c, device);
+    ck(cudaMalloc(&p, sz), what);
+  }
+  return p;
+}
+
+void deviceRelease(int device, void* p, size_t bytes) {
+  using namespace blockcache;
+  if (!p) return;
+  const size_t sz = sizeClass(bytes);
+  BlockCache& c = blockCache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  if (c.cached[device] + sz > kCacheCap) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    cudaFree(p);
+    cudaSetDevice(cur);
+    return;
+  }
+  c.blocks[{device, sz}].push_back(p);
+  c.cached[device] += sz;
+}
 
 std::vector<double> hostRates(const LoweredSystem& L, const std::vector<dcomp>& psi) {
   std::vector<double> r(L.jumps.size());
@@ -209,11 +297,43 @@ void buildSystemDevice(cqg_system& s) {
   }
   const auto& H = L.ham;
   const int S = H.S;
+  // Interaction-picture frequencies as a table of their distinct nonzero values (compared
+  // bit for bit) and an index per slot and row (kNoPhase for a zero frequency), when there
+  // are at most kPhaseTableMax distinct values: the kernels then form one exponential per
+  // value instead of one per row and slot.
+  std::vector<dcomp> fDist;
+  std::vector<unsigned short> fIdx;
+  if (!H.freq.empty()) {
+    std::map<std::pair<uint64_t, uint64_t>, int> seen;
+    fIdx.resize(H.freq.size());
+    for (size_t i = 0; i < H.freq.size(); ++i) {
+      const double re = H.freq[i].real(), im = H.freq[i].imag();
+      if (re == 0. && im == 0.) {
+        fIdx[i] = dev::kNoPhase;
+        continue;
+      }
+      std::pair<uint64_t, uint64_t> key;
+      std::memcpy(&key.first, &re, 8);
+      std::memcpy(&key.second, &im, 8);
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        if (fDist.size() == size_t(dev::kPhaseTableMax)) {
+          fDist.clear();
+          fIdx.clear();
+          break;
+        }
+        it = seen.emplace(key, int(fDist.size())).first;
+        fDist.push_back(H.freq[i]);
+      }
+      fIdx[i] = static_cast<unsigned short>(it->second);
+    }
+  }
   const size_t oCol = A.add(H.col.size() * 4 + 4), oJcol = A.add(jcol.size() * 4 + 4), oJw = A.add(jw.size() * 8 + 8),
                oJHasW = A.add(jHasW.size() * 4 + 4), oOcol = A.add(ocol.size() * 4 + 4),
                oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4), oOS = A.add(oS.size() * 4 + 4),
                oOF = A.add(oF.size() * 4 + 4), oFW = A.add(L.fourierW.size() * 8 + 8),
                oFreq = A.add(H.freq.size() * 16 + 16), oLambda = A.add(L.lambda.size() * 16 + 16),
+               oFIdx = A.add(fIdx.size() * 2 + 16), oFDist = A.add(fDist.size() * 16 + 16),
                oDiagD = A.add(H.diag.size() * 16 + 16), oValD = A.add(H.val.size() * 16 + 16),
                oJvalD = A.add(jval.size() * 16 + 16), oDiagF = A.add(H.diag.size() * 8 + 8),
                oValF = A.add(H.val.size() * 8 + 8), oJvalF = A.add(jval.size() * 8 + 8);
@@ -231,6 +351,8 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oOF, oF);
   upload(b, oFW, L.fourierW);
   upload(b, oFreq, toD2(H.freq));
+  upload(b, oFIdx, fIdx);
+  upload(b, oFDist, toD2(fDist));
   upload(b, oLambda, toD2(L.lambda));
   upload(b, oDiagD, toD2(H.diag));
   upload(b, oValD, toD2(H.val));
@@ -267,6 +389,9 @@ void buildSystemDevice(cqg_system& s) {
   while ((int64_t(1) << sd.fLog2) < L.fourierN) ++sd.fLog2;
   for (int k = 0; k < 4; ++k) sd.fObs[k] = k < sd.nF ? L.fourierObs[size_t(k)] : -1;
   sd.freq = H.freq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFreq);
+  sd.nFD = int(fDist.size());
+  sd.fIdx = fIdx.empty() ? nullptr : reinterpret_cast<const unsigned short*>(b + oFIdx);
+  sd.fDist = fDist.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFDist);
   sd.lambda = L.lambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oLambda);
   sd.diagD = reinterpret_cast<const double2*>(b + oDiagD);
   sd.valD = reinterpret_cast<const double2*>(b + oValD);
@@ -401,7 +526,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
                oRng = A.add(nTraj * 32), oCnt = A.add(nTraj * 64), oMax = A.add(nTraj * 24), oSt = A.add(nTraj * 4),
                oJT = A.add(nTraj * e->jumpCap * 8), oJL = A.add(nTraj * e->jumpCap * 4), oJN = A.add(nTraj * 8),
                oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(kMaxGroups * sizeof(int)), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
-  ck(cudaMalloc(&e->dmem, A.total), "cudaMalloc(ensemble)");
+  e->dmem = deviceAlloc(A.total, "cudaMalloc(ensemble)");
+  e->dmemBytes = A.total;
   char* b = static_cast<char*>(e->dmem);
 
   // Host image of the arena's first part (states, offsets, indices, times, random streams,
@@ -511,6 +637,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       g.Dmax = std::max<int>(g.Dmax, int(s->L.D));
       g.smax = std::max(g.smax, s->sd.S);
       g.anyFreq |= s->sd.hasFreq != 0;
+      g.phaseElems = std::max(g.phaseElems, blockPhaseElems(s->sd));
     }
     g.count = k - g.first;
     e->groups.push_back(g);
@@ -525,6 +652,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 512 : 128))
       return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 512");
     g.smemVectors = pars->cta_threads > 0 && pars->cta_shared_vectors && sharedVectorsFit(g, e->elemBytes, e->device);
+    g.phaseTable = pars->ip_phase_table >= 0;
+    if (!g.phaseTable || g.kind == 0) g.phaseElems = 0;
   }
   if (pars->autotune && pars->cta_threads <= 0)
     for (size_t gi = 0; gi < e->groups.size(); ++gi) {
@@ -547,10 +676,10 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
   if (g.kind == 0) {
     KernelFn fn = pickKernel(fp64, g.E, g.smax, g.anyFreq);
     const int warps = g.threads / 32;
-    // stage vectors, warp scratch, and for interaction-picture systems the phase cache
-    ra.phaseCache = g.anyFreq ? 1 : 0;
+    // stage vectors, warp scratch, and for interaction-picture systems the phase tables
+    ra.phaseCache = g.anyFreq && g.phaseTable ? 1 : 0;
     const size_t smem = size_t(warps) * 3 * 32 * g.E * elemBytes + size_t(warps) * sizeof(dev::WarpScratch) +
-                        (g.anyFreq ? size_t(warps) * warpSlotInstance(g.smax) * 32 * g.E * sizeof(double2) : 0);
+                        (ra.phaseCache ? size_t(warps) * dev::kWarpPhaseElems * sizeof(double2) : 0);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -566,7 +695,13 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
     // per-CTA scratch slab or, when the group says so, in shared memory too
     dev::BlockKernelFn fn = dev::pick_block(fp64, g.anyFreq);
     int smemD = g.Dmax;
-    const size_t smem = blockSmemBytes(g.Dmax, elemBytes, g.smemVectors);
+    if (g.phaseElems > 0) {  // a phase table that does not fit leaves the phases per row and slot
+      int device = 0, optin = 0;
+      ck(cudaGetDevice(&device), "cudaGetDevice");
+      ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
+      if (blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems) > size_t(optin)) g.phaseElems = 0;
+    }
+    const size_t smem = blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -577,15 +712,19 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
     dev::BlockScratch bsc;
     bsc.stride = (g.Dmax + 31) / 32 * 32;
     bsc.base = nullptr;
+    bsc.phaseElems = g.phaseElems;
     if (!g.smemVectors) {
       const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * elemBytes;
       if (need > g.scratchBytes) {
+        int device = 0;
+        ck(cudaGetDevice(&device), "cudaGetDevice");
         if (g.scratch) {
           ck(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-          cudaFree(g.scratch);
+          deviceRelease(device, g.scratch, g.scratchBytes);
         }
         g.scratch = nullptr;
-        ck(cudaMalloc(&g.scratch, need), "cudaMalloc(block scratch)");
+        g.scratchBytes = 0;
+        g.scratch = deviceAlloc(need, "cudaMalloc(block scratch)");
         g.scratchBytes = need;
       }
       bsc.base = g.scratch;
@@ -606,16 +745,20 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   const int nAvr = e->nAvrMax + 1;  // the linear averages, then dtDid
   const size_t need = size_t(std::max(nOut, 1)) * e->nTraj * nAvr;
   if (need > e->avrCap) {
-    if (e->dAvr) cudaFree(e->dAvr);
+    ck(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    cqg::engine::deviceRelease(e->device, e->dAvr, e->avrCap * sizeof(double));
     e->dAvr = nullptr;
-    ck(cudaMalloc(&e->dAvr, need * sizeof(double)), "cudaMalloc(averages)");
+    e->avrCap = 0;
+    e->dAvr = static_cast<double*>(cqg::engine::deviceAlloc(need * sizeof(double), "cudaMalloc(averages)"));
     e->avrCap = need;
   }
   const size_t needS = size_t(std::max(nOut, 1)) * nAvr;
   if (needS > e->sumsCap) {
-    if (e->dSums) cudaFree(e->dSums);
+    ck(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    cqg::engine::deviceRelease(e->device, e->dSums, e->sumsCap * sizeof(double));
     e->dSums = nullptr;
-    ck(cudaMalloc(&e->dSums, needS * sizeof(double)), "cudaMalloc(sums)");
+    e->sumsCap = 0;
+    e->dSums = static_cast<double*>(cqg::engine::deviceAlloc(needS * sizeof(double), "cudaMalloc(sums)"));
     e->sumsCap = needS;
   }
   ck(cudaEventRecord(e->evRun0, e->stream), "cudaEventRecord");
@@ -702,7 +845,7 @@ std::vector<int> threadCandidates(const KernelGroup& g, bool vectorsFit) {
 bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device) {
   int optin = 0;
   ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
-  return g.kind == 1 && blockSmemBytes(g.Dmax, elemBytes, true) <= size_t(optin);
+  return g.kind == 1 && blockSmemBytes(g.Dmax, elemBytes, true, g.phaseElems) <= size_t(optin);
 }
 
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,

@@ -35,6 +35,12 @@ struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// Recycled device blocks (api.cu): ensemble buffers come from and go back to a per-device
+// cache instead of cudaMalloc / cudaFree.  deviceAlloc allocates on the current device;
+// deviceRelease takes the device the block lives on and the size it was requested with.
+void* deviceAlloc(size_t bytes, const char* what);
+void deviceRelease(int device, void* p, size_t bytes);
+
 inline void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -75,6 +81,9 @@ struct KernelGroup {
   int Dmax = 0;
   bool anyFreq = false;  // some system of the group has interaction-picture frequencies
   bool smemVectors = false;  // CTA kind: stage derivatives in shared memory instead of scratch
+  bool phaseTable = true;    // interaction picture: phases from the systems' tables of
+                             // distinct frequencies where they have one
+  int phaseElems = 0;        // CTA kind: shared-memory phase table capacity (max over systems)
   int threads = 0;  // CTA size
   int64_t first = 0, count = 0;
   cudaStream_t stream = nullptr;
@@ -86,12 +95,16 @@ struct KernelGroup {
 inline int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
 
 // Dynamic shared memory of the CTA kernel: two stage vectors of Dmax elements, the reduction
-// scratch and broadcast words, and with shared-memory vectors the kBlockVectors stage
-// derivatives / candidate / cache of ceil32(Dmax) elements each.
-inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors) {
-  const size_t base = 2 * size_t(Dmax) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64;
+// scratch and broadcast words, the interaction-picture phase table of phaseElems double2,
+// and with shared-memory vectors the kBlockVectors stage derivatives / candidate / cache of
+// ceil32(Dmax) elements each.
+inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors, int phaseElems) {
+  const size_t base = 2 * size_t(Dmax) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64 +
+                      size_t(phaseElems) * sizeof(double2);
   return base + (vectors ? size_t(dev::kBlockVectors) * size_t((Dmax + 31) / 32 * 32) * elemBytes : 0);
 }
+// Phase-table capacity a CTA-kernel group needs for one of its systems
+inline int blockPhaseElems(const dev::SysDev& sd) { return sd.hasFreq && sd.fIdx ? sd.nFD : 0; }
 
 // the off-diagonal slot bound of the warp kernel instance that serves smax slots
 inline int warpSlotInstance(int smax) { return smax <= 2 ? 2 : smax <= 4 ? 4 : 8; }

@@ -31,6 +31,7 @@ struct BlockScratch {
   void* base;           // [gridDim.x][kBlockVectors][stride] Real2, or null: the vectors
                         // follow the broadcast words in dynamic shared memory
   long long stride;     // elements per vector (>= max D)
+  int phaseElems;       // IP: capacity of the shared-memory phase table (0: none)
 };
 
 // block-wide sums of n <= N uniform values; red holds 32 * N doubles of shared memory
@@ -75,6 +76,10 @@ struct BlockWorker {
   const C2* val;
   const C2* diag;
   const double2* freq;
+  const unsigned short* fIdx;  // IP: distinct-frequency index per slot and row, or null
+  const double2* fDist;
+  int nFD;
+  double2* phTab;  // IP: shared-memory phases of the distinct frequencies, or null
   C2* x;       // the trajectory's state (device memory)
   C2* vec;     // this CTA's scratch vectors
   long long stride;
@@ -96,12 +101,29 @@ struct BlockWorker {
   // out = (H/i) y at picture time tau, y in shared memory
   __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
     ++nRhs;
+    bool tab = false;
+    if constexpr (IP) {
+      // exp(tau f) once per distinct frequency into shared memory: the same values, bit for
+      // bit, as one exponential per row and slot
+      tab = phTab && hasFreq && tau != 0.;
+      if (tab) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < nFD; k += blockDim.x) phTab[k] = cexpScaled(tau, __ldg(&fDist[k]));
+        __syncthreads();
+      }
+    }
     for (int r = threadIdx.x; r < D; r += blockDim.x) {
       C2 acc = cmul(diag[r], ys[r]);
       for (int s = 0; s < S; ++s) {
         C2 c = __ldg(&val[s * D + r]);
         if constexpr (IP) {
-          if (hasFreq && tau != 0.) {  // exp(0 f) = 1 exactly
+          if (tab) {
+            const unsigned k = __ldg(&fIdx[s * D + r]);
+            if (k != kNoPhase) {
+              const double2 ph = phTab[k];
+              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+            }
+          } else if (hasFreq && tau != 0.) {  // exp(0 f) = 1 exactly
             const double2 f = __ldg(&freq[s * D + r]);
             if (f.x != 0. || f.y != 0.) {
               const double2 ph = cexpScaled(tau, f);
@@ -510,7 +532,8 @@ struct BlockWorker {
 };
 
 // Dynamic shared memory: two stage buffers of `smemD` elements, the reduction scratch,
-// then 8 broadcast words.
+// 8 broadcast words, the interaction-picture phase table (bsc.phaseElems double2), then
+// (without a scratch slab) the stage derivatives.
 template <typename R, bool IP>
 __global__ void __launch_bounds__(512, 1) mcwfBlockKernel(TrajDev td, RunArgs ra, BlockScratch bsc, int smemD) {
   using C2 = typename CT<R>::T;
@@ -540,8 +563,14 @@ __global__ void __launch_bounds__(512, 1) mcwfBlockKernel(TrajDev td, RunArgs ra
     w.val = Tables<R>::val(*s);
     w.diag = Tables<R>::diag(*s);
     w.freq = s->freq;
+    // the phase table follows the broadcast words; shared-memory vectors follow the table
+    double2* phTab = reinterpret_cast<double2*>(bcast + 8);
+    w.fIdx = s->fIdx;
+    w.fDist = s->fDist;
+    w.nFD = s->nFD;
+    w.phTab = IP && s->fIdx && s->nFD <= bsc.phaseElems ? phTab : nullptr;
     w.vec = bsc.base ? reinterpret_cast<C2*>(bsc.base) + size_t(blockIdx.x) * kBlockVectors * bsc.stride
-                     : reinterpret_cast<C2*>(bcast + 8);
+                     : reinterpret_cast<C2*>(phTab + bsc.phaseElems);
     w.stride = bsc.stride;
     w.ys0 = ys0;
     w.ys1 = ys1;

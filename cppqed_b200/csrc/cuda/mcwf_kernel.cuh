@@ -23,6 +23,15 @@ namespace cqg {
 namespace dev {
 
 constexpr int MAX_JUMPS = 8;
+// Interaction-picture frequency tables: a system's distinct nonzero frequencies when there
+// are at most kPhaseTableMax of them (the CTA kernel's shared-memory table); the warp kernel
+// uses a table of at most kWarpPhaseTableMax.  kNoPhase indexes a zero frequency.
+constexpr int kPhaseTableMax = 1024;
+constexpr int kWarpPhaseTableMax = 128;
+constexpr unsigned short kNoPhase = 0xffff;
+// per-warp phase region of the warp kernel (double2 elements): the five Cash-Karp stage
+// phases of each distinct frequency of the table, stage-major
+constexpr int kWarpPhaseElems = 5 * kWarpPhaseTableMax;
 constexpr unsigned FULL = 0xffffffffu;
 
 // ---- complex helpers ---------------------------------------------------------
@@ -88,21 +97,22 @@ static __device__ __noinline__ double2 cexpScaled(double tau, double2 f) {
   return make_double2(m * c, m * s);
 }
 
+// complex product with explicit roundings (no contraction choices left to the compiler)
 __device__ __forceinline__ double2 cmulD(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_double2(__fma_rn(a.x, b.x, -__dmul_rn(a.y, b.y)), __fma_rn(a.x, b.y, __dmul_rn(a.y, b.x)));
 }
 // Interaction-picture phases of the Cash-Karp stages from one exponential per attempt: with
 // E = exp(dt f / 40), stage s (c_s = 1/5, 3/10, 3/5, 1, 7/8) needs exp(c_s dt f) = E^n,
 // n = 8, 12, 24, 40, 35, by repeated squaring (relative error ~ n ulp).
-__device__ __forceinline__ double2 stagePhase(double2 E, int stage) {
+__device__ __forceinline__ void stagePhases(double2 E, double2* out, int stride) {
   const double2 e2 = cmulD(E, E), e4 = cmulD(e2, e2), e8 = cmulD(e4, e4);
-  if (stage == 1) return e8;
   const double2 e12 = cmulD(e8, e4);
-  if (stage == 2) return e12;
-  if (stage == 3) return cmulD(e12, e12);
   const double2 e16 = cmulD(e8, e8), e32 = cmulD(e16, e16);
-  if (stage == 4) return cmulD(e32, e8);
-  return cmulD(cmulD(e32, e2), E);
+  out[0] = e8;
+  out[stride] = e12;
+  out[2 * stride] = cmulD(e12, e12);
+  out[3 * stride] = cmulD(e32, e8);
+  out[4 * stride] = cmulD(cmulD(e32, e2), E);
 }
 
 // ---- warp reductions -----------------------------------------------------------
@@ -193,6 +203,9 @@ struct SysDev {
   const int* oFourier;   // [nObs] 1: evaluated by the transform (CTA kernel), else 0
   const double* fW;      // [nF][fN] weights
   const double2* freq;   // [S][D] (IP) or null
+  int nFD;               // IP with a table: distinct nonzero values of freq
+  const unsigned short* fIdx;  // [S][D] index of freq into fDist (kNoPhase: zero), or null
+  const double2* fDist;  // [nFD]
   const double2* lambda; // [D] (Exact) or null
   // precision-specific copies
   const double2* diagD;
@@ -261,7 +274,7 @@ struct RunArgs {
   int* queue;
   const int* order;  // the launch's trajectories (a segment of the ensemble's order)
   int nTasks;        // how many
-  int phaseCache;    // shared memory holds a per-warp interaction-picture phase cache
+  int phaseCache;    // warp kernel: shared memory holds a per-warp interaction-picture phase table
 };
 
 // Cash-Karp tableau (published coefficients)
@@ -303,8 +316,10 @@ struct Worker {
   C2* buf1;
   C2* cache;
   WarpScratch* ws;
-  double2* phs;  // per-warp phase cache [SMAX][32 E] or null
+  double2* phs;  // per-warp phase region [5][kWarpPhaseTableMax] or null
   bool phsOn;    // this attempt's stage phases come from phs
+  bool phsTab;   // the system's distinct frequencies fit the per-warp table
+  const unsigned short* fIdx;  // with phsTab: distinct-frequency index per slot and row
 
   // Coefficients live in registers when E * SMAX is small (CREG), else they are
   // re-read per right-hand side through L1 (shared by all trajectories of the system).
@@ -328,7 +343,7 @@ struct Worker {
 
   __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w,
                                     double2* ph)
-      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w), phs(ph), phsOn(false) {
+      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w), phs(ph), phsOn(false), phsTab(false) {
     D = s->D;
     S = s->S;
     nJ = s->nJ;
@@ -338,6 +353,8 @@ struct Worker {
     col = s->col;
     val = Tables<R>::val(*s);
     freq = s->freq;
+    phsTab = ph && s->fIdx && s->nFD <= kWarpPhaseTableMax;
+    fIdx = s->fIdx;
     jw = s->jw;
     anySpecial = false;
     for (int m = 0; m < nJ; ++m) anySpecial |= !s->jHasW[m];
@@ -375,22 +392,23 @@ struct Worker {
     }
   }
 
-  // out = (H/i) y at picture time tau; y staged through `buf`
-  // E = exp(dt f / 40) of every row and slot for this attempt (t == t0: the stage times are
-  // c_s dt past the picture's reference time)
+  // The stage phases exp(c_s dt f) of this attempt for every distinct frequency f of the
+  // system (t == t0: the stage times are c_s dt past the picture's reference time): lane k
+  // takes frequencies k, k + 32, ..., forms E = exp(dt f / 40) and its stage powers.  One
+  // shared table per warp keeps the unrolled right-hand sides small (a per-row-and-slot phase
+  // path beside it overflowed the instruction cache: ncu no_instruction stalls 2.7 -> 6.5
+  // per issued instruction).
   __device__ __forceinline__ void preparePhases(double dt) {
     const double q = dt / 40.;
-#pragma unroll
-    for (int e = 0; e < E; ++e)
-      if (valid(e)) {
-#pragma unroll
-        for (int s = 0; s < SMAX; ++s)
-          if (s < S) {
-            const double2 f = __ldg(&freq[s * D + row(e)]);
-            phs[s * 32 * E + row(e)] = (f.x != 0. || f.y != 0.) ? cexpScaled(q, f) : make_double2(1., 0.);
-          }
-      }
+    __syncwarp();  // every lane is done with the previous attempt's table
+    for (int k = lane; k < sysp->nFD; k += 32) {
+      const double2 f = __ldg(&sysp->fDist[k]);
+      stagePhases(cexpScaled(q, f), phs + k, kWarpPhaseTableMax);
+    }
+    __syncwarp();
   }
+
+  // out = (H/i) y at picture time tau; y staged through `buf`
 
   // out = (H/i) y at picture time tau = stage time - t0 (stage 0..5 of the attempt)
   __device__ __forceinline__ void rhs(const C2 (&y)[E], C2 (&out)[E], double tau, int stage, C2* buf) {
@@ -418,7 +436,8 @@ struct Worker {
           if (IP && hasFreq && valid(e)) {
             if (phsOn) {
               if (stage) {
-                const double2 ph = stagePhase(phs[s * 32 * E + r], stage);
+                const unsigned k = __ldg(&fIdx[s * D + r]);
+                const double2 ph = k == kNoPhase ? make_double2(1., 0.) : phs[(stage - 1) * kWarpPhaseTableMax + k];
                 c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
               }
             } else {
@@ -453,7 +472,7 @@ struct Worker {
       ++nAttempts;
       const double dt = dtTry;
       if constexpr (IP) {
-        phsOn = phs && hasFreq && t == t0;
+        phsOn = phsTab && hasFreq && t == t0;
         if (phsOn) preparePhases(dt);
       }
       {
@@ -857,11 +876,11 @@ __global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td
   C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * 3 * DMAX;
   WarpScratch* ws =
       reinterpret_cast<WarpScratch*>(smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) + warp;
-  // optional phase cache after every warp's scratch: [warps][SMAX][DMAX] double2
+  // optional phase tables after every warp's scratch: [warps][kWarpPhaseElems] double2
   double2* phs = IP && ra.phaseCache ? reinterpret_cast<double2*>(reinterpret_cast<WarpScratch*>(
                                      smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) +
                                  blockDim.x / 32) +
-                                     size_t(warp) * SMAX * DMAX
+                                     size_t(warp) * kWarpPhaseElems
                                : nullptr;
   while (true) {
     int task = 0;

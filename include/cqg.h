@@ -153,7 +153,12 @@ typedef struct cqg_mcwf_pars {
   int32_t cta_shared_vectors;  /* with cta_threads > 0, for CTA-per-trajectory groups: 1 keeps
                                   the stage derivatives in shared memory (when they fit), 0 in
                                   a global scratch slab; the autotuner chooses otherwise */
-  int32_t reserved;
+  int32_t ip_phase_table;      /* interaction-picture phases exp(tau f) of the off-diagonal
+                                  terms: 0 forms them once per distinct frequency f of the
+                                  system (at most 128 on the warp kernel: per attempt, the
+                                  stage powers of exp(dt f / 40); at most 1024 on the CTA
+                                  kernel: per stage, bit-identical to -1), -1 forms them per
+                                  row, slot and stage as the reference does */
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);

@@ -436,6 +436,66 @@ def test_block_kernel_cta_shapes_agree(gpu):
         assert agree >= n - 1
 
 
+IP_TABLE_CASES = [
+    # (script, args, kernel kind) interaction-picture systems: on the warp kernel qubit-mode
+    # JC 2x40 (E = 3, a few distinct frequencies), pumped lossy mode (E = 1), optomechanics
+    # 4 x 12 (E = 2); on the CTA kernel a particle in a cavity 8 x 32 (momentum-dependent
+    # frequencies) and optomechanics 20 x 60
+    ("QbitMode_C++QED", ["--picture", "IP", "--deltaA", "-1", "--gamma", "0.5", "--deltaC", "2", "--kappa", "1",
+                         "--eta", "1.5", "--cutoff", "40", "--g", "2"], 0),
+    ("PumpedLossyMode_C++QED", ["--picture", "IP", "--deltaC", "-1", "--eta", "2", "--kappa", "1", "--cutoff", "30",
+                                "--no_quadratures"], 0),
+    ("Optomechanics", ["--picture", "IP", "--cutoffOpt", "4", "--cutoffMech", "12", "--kappaOpt", "1",
+                       "--etaOpt", "1", "--deltaCOpt", "-1", "--deltaCMech", "-2", "--u", "0.1"], 0),
+    ("1particle1mode", ["--1p1mconf", "2", "--vClass", "0", "--modeCav", "Cos", "--kCav", "1", "--Unot", "-1",
+                        "--eta", "5", "--kappa", "1", "--cutoff", "8", "--fin", "5"], 1),
+    ("Optomechanics", ["--picture", "IP", "--cutoffOpt", "20", "--cutoffMech", "60", "--kappaOpt", "1",
+                       "--etaOpt", "1", "--deltaCOpt", "-1", "--deltaCMech", "-2", "--u", "0.1"], 1),
+]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("case", range(len(IP_TABLE_CASES)))
+def test_ip_phase_table_matches_per_row_phases(gpu, case, precision):
+    """Interaction-picture phases from the table of distinct frequencies against the phases
+    formed per row, slot and stage (ip_phase_table = -1, the reference's arithmetic).  On the
+    CTA kernel the table holds exp(tau f) per stage: the same bits.  On the warp kernel it
+    holds the stage powers of exp(dt f / 40) (a few ulp from exp(c_s dt f)): the same
+    trajectories up to rounding."""
+    script, args, kind = IP_TABLE_CASES[case]
+    model = gpu.Model(script, args)
+    sysd = gpu.System(model.desc)
+    n = 96 if kind == 0 else 12
+    out = []
+    for table in (0, -1):
+        pars = model.run_pars().mcwf
+        pars.precision = A.FP64 if precision == "fp64" else A.FP32
+        pars.ip_phase_table = table
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        assert ens.plan()[0]["kind"] == kind
+        sums = ens.run(0.4 if kind == 0 else 0.1, 2)
+        out.append((sums, np.stack([ens.state(i, model.dim) for i in range(n)]), ens.times(), ens.counters(),
+                    [ens.jumps(i) for i in range(n)]))
+    (s0, x0, t0, c0, j0), (s1, x1, t1, c1, j1) = out
+    if script != "Optomechanics" or kind == 0:  # the large optomechanics case is too short for jumps
+        assert c0[:, 6].sum() > 0
+    if kind == 1:
+        assert np.array_equal(x0, x1)
+        assert np.array_equal(s0, s1)
+        for a, b in zip(t0, t1):
+            assert np.array_equal(a, b)
+        assert np.array_equal(c0, c1)
+        return
+    tol, rt = (1e-9, 1e-8) if precision == "fp64" else (2e-4, 1e-4)
+    agree = 0
+    for i in range(n):
+        (ta, la), (tb, lb) = j0[i], j1[i]
+        if len(ta) == len(tb) and np.allclose(ta, tb, rtol=rt) and np.array_equal(la, lb):
+            agree += 1
+            assert np.linalg.norm(x0[i] - x1[i]) < tol
+    assert agree >= n - 2
+
+
 # ---- particle in a cavity on the CTA-per-trajectory kernel ----
 
 PARTICLE_ARGS = ["--1p1mconf", "2", "--vClass", "0", "--modeCav", "Cos", "--kCav", "1", "--Unot", "-1",
