@@ -112,26 +112,36 @@ struct BlockWorker {
         __syncthreads();
       }
     }
+    // The operator tables are shared by all trajectories and live in L2 (L1 is mostly given
+    // to shared memory here).  The slot loops are unrolled by four and free of calls, so that
+    // the loads of several slots are in flight together; the products are accumulated in
+    // slot order in every variant.
     for (int r = threadIdx.x; r < D; r += blockDim.x) {
       C2 acc = cmul(diag[r], ys[r]);
-      for (int s = 0; s < S; ++s) {
-        C2 c = __ldg(&val[s * D + r]);
-        if constexpr (IP) {
-          if (tab) {
-            const unsigned k = __ldg(&fIdx[s * D + r]);
-            if (k != kNoPhase) {
-              const double2 ph = phTab[k];
-              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
-            }
-          } else if (hasFreq && tau != 0.) {  // exp(0 f) = 1 exactly
-            const double2 f = __ldg(&freq[s * D + r]);
-            if (f.x != 0. || f.y != 0.) {
-              const double2 ph = cexpScaled(tau, f);
-              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
-            }
+      if (IP && tab) {
+#pragma unroll 4
+        for (int s = 0; s < S; ++s) {
+          C2 c = __ldg(&val[s * D + r]);
+          const unsigned k = __ldg(&fIdx[s * D + r]);
+          if (k != kNoPhase) {
+            const double2 ph = phTab[k];
+            c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
           }
+          acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
         }
-        acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
+      } else if (IP && hasFreq && tau != 0.) {
+        for (int s = 0; s < S; ++s) {
+          C2 c = __ldg(&val[s * D + r]);
+          const double2 f = __ldg(&freq[s * D + r]);
+          if (f.x != 0. || f.y != 0.) {  // exp(0 f) = 1 exactly
+            const double2 ph = cexpScaled(tau, f);
+            c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+          }
+          acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
+        }
+      } else {
+#pragma unroll 4
+        for (int s = 0; s < S; ++s) acc = cfma(__ldg(&val[s * D + r]), ys[__ldg(&col[s * D + r])], acc);
       }
       out[r] = acc;
     }
