@@ -334,7 +334,11 @@ def run_ours(args, rank, world, dev):
     value = steps_total / (run_ms_max * 1e-3)
 
     # end to end through the public API from host buffers: create (upload of the host
-    # states), one Dt interval, read-back of the averages, destroy
+    # states), one Dt interval, read-back of the averages, destroy; one untimed call first,
+    # as for the device-timed steps (first-use allocations of the engine's buffers)
+    e = cqg.Ensemble(system, psi0, n_traj, pars)
+    allreduce(e.run(Dt, 1))
+    del e
     e2e_steps = 0
     phases = np.zeros(4)  # create (host states uploaded), run (one Dt, sums read back), counters, destroy
     t0 = time.perf_counter()
@@ -465,14 +469,20 @@ def run_batched(args, dev):
         del e
     plain_value = p_steps / (p_ms * 1e-3)
 
-    # end to end: batch created from host states, one Dt, averages read back
-    t0 = time.perf_counter()
+    # end to end: batch created from host states, one Dt, averages read back, destroyed;
+    # one untimed call first (first-use allocations), then three timed calls
     e = cqg.Ensemble.batch(systems, idx, psi0s, pars_for(precision))
     e.run(Dt, 1)
-    e2e_steps = int(e.counters()[:, 0].sum())
+    del e
+    e2e_steps = 0
+    t0 = time.perf_counter()
+    for _ in range(3):
+        e = cqg.Ensemble.batch(systems, idx, psi0s, pars_for(precision))
+        e.run(Dt, 1)
+        e2e_steps += int(e.counters()[:, 0].sum())
+        del e
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
-    del e
     dims = np.array([m.dim for m in models])[idx]
     out = {"metric": "MCWF trajectory-steps/s", "value": value, "unit": "trajectory-steps/s", "n_gpus": 1,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r_ms / args.steps, "higher_is_better": True,

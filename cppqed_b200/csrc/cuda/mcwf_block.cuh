@@ -164,9 +164,14 @@ struct BlockWorker {
       const double dt = dtTry;
       for (int st = 1; st <= 5; ++st) {
         C2* ys = (st & 1) ? ys1 : ys0;
+        R a[5];  // this stage's tableau row times dt (unrolled below: all loads of a row at once)
+#pragma unroll
+        for (int j = 0; j < 5; ++j) a[j] = j < st ? R(dt * kBlockA[st - 1][j]) : R(0);
         for (int r = threadIdx.x; r < D; r += blockDim.x) {
           C2 y = x[r];
-          for (int j = 0; j < st; ++j) y = axpy(R(dt * kBlockA[st - 1][j]), K(j)[r], y);
+#pragma unroll
+          for (int j = 0; j < 5; ++j)
+            if (j < st) y = axpy(a[j], K(j)[r], y);
           ys[r] = y;
         }
         __syncthreads();
