@@ -358,7 +358,10 @@ def run_ours(args, rank, world, dev):
     e2e_tot = allreduce(np.array([e2e_steps, e2e_s], dtype=np.float64))
     e2e_s = float(sharding.max_over_ranks([e2e_s], world)[0])
     e2e_value = float(e2e_tot[0]) / e2e_s
-    h2d = n_traj * model.dim * 16 + n_traj * (8 * 4 + 32 + 64)
+    # sent per call: the initial state once (replicated on the device), and per trajectory its
+    # slot and state offsets, system index, times, random stream and counters
+    elem = 16 if args.precision == "fp64" else 8
+    h2d = model.dim * elem + n_traj * (8 + 8 + 4 + 8 * 4 + 32 + 64)
     d2h = (model.n_avr + 1) * 8 + 4
 
     apply = run_apply(model) if rank == 0 else None
@@ -497,7 +500,9 @@ def run_batched(args, dev):
            "batched_vs_plain": value / plain_value,
            "precision_check": precision_check,
            "e2e": {"value": e2e_steps / e2e_s, "unit": "trajectory-steps/s",
-                   "h2d_bytes_per_step": int(dims.sum()) * 16, "d2h_bytes_per_step": (models[0].n_avr + 1) * 8},
+                   "h2d_bytes_per_step": sum(m.dim for m in models) * (16 if args.precision == "fp64" else 8)
+                   + n_traj * (8 + 8 + 4 + 8 * 4 + 32 + 64),
+                   "d2h_bytes_per_step": (models[0].n_avr + 1) * 8},
            "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved,
                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                         "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU"},

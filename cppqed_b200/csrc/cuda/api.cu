@@ -466,6 +466,20 @@ __global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, 
   if (threadIdx.x == 0) sums[(size_t)k * nAvr + c] = part[0];
 }
 
+// Initial states: trajectory i's slot (dimension from the slot offsets) receives a copy of its
+// distinct initial state, which the host uploaded once; 8-byte words.
+__global__ void replicateStatesKernel(const unsigned long long* __restrict__ uniq, const long long* __restrict__ uOff,
+                                      const long long* __restrict__ psiOff, long long nTraj, long long psiElems,
+                                      int wordsPerElem, unsigned long long* __restrict__ psi) {
+  for (long long i = blockIdx.x; i < nTraj; i += gridDim.x) {
+    const long long D = (i + 1 < nTraj ? psiOff[i + 1] : psiElems) - psiOff[i];
+    const long long n = D * wordsPerElem;
+    const unsigned long long* src = uniq + uOff[i] * wordsPerElem;
+    unsigned long long* dst = psi + psiOff[i] * wordsPerElem;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) dst[k] = src[k];
+  }
+}
+
 __global__ void statusOrKernel(const unsigned* __restrict__ st, int n, unsigned* out) {
   unsigned v = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v |= st[i];
@@ -520,56 +534,96 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
   }
   const long long psiElems = off;
 
+  // Distinct initial states: one for a single-state ensemble, one per distinct (offset,
+  // dimension) in a batch.  Each is converted and sent once; a kernel copies it into the
+  // slots of its trajectories.
+  std::vector<int> uId(nTraj);          // trajectory i's distinct state
+  std::vector<long long> uOff(nTraj);   // element offset of trajectory i's state in the list
+  std::vector<int64_t> uFirst;          // a trajectory of each distinct state
+  std::vector<long long> uStart;        // element offset of each distinct state in the list
+  long long uniqElems = 0;
+  if (!psi0Off && nSys == 1) {  // one state for the whole ensemble
+    uFirst.push_back(0);
+    uStart.push_back(0);
+    uniqElems = systems[0]->L.D;
+  } else {
+    std::map<std::pair<int64_t, int64_t>, int> seen;
+    for (int64_t i = 0; i < nTraj; ++i) {
+      const int64_t D = systems[e->sysIdx[i]]->L.D;
+      const std::pair<int64_t, int64_t> key(psi0Off ? psi0Off[i] : 0, D);
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        it = seen.emplace(key, int(uFirst.size())).first;
+        uFirst.push_back(i);
+        uStart.push_back(uniqElems);
+        uniqElems += D;
+      }
+      uId[i] = it->second;
+    }
+  }
+  for (int64_t i = 0; i < nTraj; ++i) uOff[i] = uStart[size_t(uId[i])];
+
   Arena A;
   const size_t oPsi = A.add(size_t(psiElems) * e->elemBytes), oOff = A.add(nTraj * 8), oIdx = A.add(nTraj * 4),
                oT = A.add(nTraj * 8), oT0 = A.add(nTraj * 8), oTry = A.add(nTraj * 8), oDid = A.add(nTraj * 8),
-               oRng = A.add(nTraj * 32), oCnt = A.add(nTraj * 64), oMax = A.add(nTraj * 24), oSt = A.add(nTraj * 4),
+               oRng = A.add(nTraj * 32), oCnt = A.add(nTraj * 64), oUOff = A.add(nTraj * 8),
+               oUniq = A.add(size_t(uniqElems) * e->elemBytes), oMax = A.add(nTraj * 24), oSt = A.add(nTraj * 4),
                oJT = A.add(nTraj * e->jumpCap * 8), oJL = A.add(nTraj * e->jumpCap * 4), oJN = A.add(nTraj * 8),
                oSys = A.add(nSys * sizeof(dev::SysDev)), oQ = A.add(kMaxGroups * sizeof(int)), oOrd = A.add(nTraj * 4), oSOr = A.add(16);
   e->dmem = deviceAlloc(A.total, "cudaMalloc(ensemble)");
   e->dmemBytes = A.total;
   char* b = static_cast<char*>(e->dmem);
 
-  // Host image of the arena's first part (states, offsets, indices, times, random streams,
-  // counters) in a pinned staging buffer, sent in one copy; the rest is zeroed on the device.
+  // Host image of the arena from the slot offsets to the distinct initial states (offsets,
+  // indices, times, random streams, counters, the states) in a pinned staging buffer, sent in
+  // one copy; the trajectories' slots are filled on the device, the rest is zeroed there.
   {  // the staging buffer is held only for this block (the autotuner below creates ensembles)
-  HostStaging staging(oMax);
-  char* h = staging.data();
+  HostStaging staging(oMax - oOff);
+  char* const h0 = staging.data();
+  auto H = [&](size_t o) { return h0 + (o - oOff); };  // host address of arena offset o
   const long long* offs = e->psiOff.data();
-  std::memcpy(h + oOff, offs, size_t(nTraj) * 8);
-  std::memcpy(h + oIdx, e->sysIdx.data(), size_t(nTraj) * 4);
-  auto* ht = reinterpret_cast<double*>(h + oT);
-  auto* ht0 = reinterpret_cast<double*>(h + oT0);
-  auto* hTry = reinterpret_cast<double*>(h + oTry);
-  auto* hDid = reinterpret_cast<double*>(h + oDid);
-  auto* hRng = reinterpret_cast<unsigned long long*>(h + oRng);
-  auto* hCnt = reinterpret_cast<unsigned long long*>(h + oCnt);
+  std::memcpy(H(oOff), offs, size_t(nTraj) * 8);
+  std::memcpy(H(oUOff), uOff.data(), size_t(nTraj) * 8);
+  std::memcpy(H(oIdx), e->sysIdx.data(), size_t(nTraj) * 4);
+  auto* ht = reinterpret_cast<double*>(H(oT));
+  auto* ht0 = reinterpret_cast<double*>(H(oT0));
+  auto* hTry = reinterpret_cast<double*>(H(oTry));
+  auto* hDid = reinterpret_cast<double*>(H(oDid));
+  auto* hRng = reinterpret_cast<unsigned long long*>(H(oRng));
+  auto* hCnt = reinterpret_cast<unsigned long long*>(H(oCnt));
   std::memset(hRng, 0, size_t(nTraj) * 32);
   std::memset(hCnt, 0, size_t(nTraj) * 64);
-  double dt0Shared = 0.;
-  bool overshotShared = false;
-  std::vector<dcomp> psi;
-  std::vector<unsigned char> one;  // the converted state of the current initial state
-  for (int64_t i = 0; i < nTraj; ++i) {
-    const cqg_system* s = systems[e->sysIdx[i]];
-    const int64_t D = s->L.D;
-    if (psi0Off || i == 0) {  // one initial state for a whole ensemble: convert it once
+  // per distinct state: the converted state and the initial dtTry (with its overshoot flag)
+  std::vector<double> uDt0(uFirst.size());
+  std::vector<char> uOvershot(uFirst.size());
+  {
+    std::vector<dcomp> psi;
+    for (size_t u = 0; u < uFirst.size(); ++u) {
+      const int64_t i = uFirst[u];
+      const cqg_system* s = systems[e->sysIdx[i]];
+      const int64_t D = s->L.D;
       const cqg_complex* p = psi0s + (psi0Off ? psi0Off[i] : 0);
       psi.resize(D);
       for (int64_t k = 0; k < D; ++k) psi[k] = dcomp(p[k].re, p[k].im);
-      one.resize(size_t(D) * e->elemBytes);
+      char* dst = H(oUniq) + size_t(uOff[i]) * e->elemBytes;
       for (int64_t k = 0; k < D; ++k) {
         if (e->elemBytes == 16) {
           const double2 v = make_double2(psi[k].real(), psi[k].imag());
-          std::memcpy(&one[k * 16], &v, 16);
+          std::memcpy(dst + k * 16, &v, 16);
         } else {
           const float2 v = make_float2(float(psi[k].real()), float(psi[k].imag()));
-          std::memcpy(&one[k * 8], &v, 8);
+          std::memcpy(dst + k * 8, &v, 8);
         }
       }
-      dt0Shared = initialDtTry(*s, psi, *pars, &overshotShared);
+      bool ov = false;
+      uDt0[u] = initialDtTry(*s, psi, *pars, &ov);
+      uOvershot[u] = ov ? 1 : 0;
     }
-    std::memcpy(h + oPsi + size_t(offs[i]) * e->elemBytes, one.data(), one.size());
+  }
+  for (int64_t i = 0; i < nTraj; ++i) {
+    const size_t u = size_t(uId[i]);
+    const double dt0Shared = uDt0[u];
+    const bool overshotShared = uOvershot[u] != 0;
     if (pars->rng == CQG_RNG_PCG64) {
       const auto g = dev::Pcg64::seeded(pars->seed, pars->prng_stream + uint64_t(i));
       hRng[4 * i + 0] = g.state.hi;
@@ -583,7 +637,16 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     hTry[i] = dt0Shared;
     hDid[i] = 0.;
   }
-  ck(cudaMemcpy(b, h, oMax, cudaMemcpyHostToDevice), "cudaMemcpy(ensemble)");
+  ck(cudaMemcpy(b + oOff, h0, oMax - oOff, cudaMemcpyHostToDevice), "cudaMemcpy(ensemble)");
+  }
+  {
+    const int grid = int(std::min<int64_t>(nTraj, 148 * 8));
+    replicateStatesKernel<<<grid, 128, 0, e->stream>>>(
+        reinterpret_cast<const unsigned long long*>(b + oUniq), reinterpret_cast<const long long*>(b + oUOff),
+        reinterpret_cast<const long long*>(b + oOff), nTraj, psiElems, int(e->elemBytes / 8),
+        reinterpret_cast<unsigned long long*>(b + oPsi));
+    ck(cudaGetLastError(), "replicateStatesKernel");
+    ck(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
   }
   ck(cudaMemset(b + oMax, 0, A.total - oMax), "cudaMemset");
   std::vector<dev::SysDev> sds;
