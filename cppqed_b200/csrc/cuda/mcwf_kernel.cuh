@@ -863,12 +863,19 @@ struct Worker {
   }
 };
 
-#ifndef CQG_MIN_BLOCKS
-#define CQG_MIN_BLOCKS 1
-#endif
+// CTAs of 128 threads the compiler must fit on one SM.  Three (at most 170 registers per
+// thread, some spills) for the Schroedinger-picture instance with three rows per lane, where
+// the 12 resident warps hide more latency than the spills cost (qubit-mode 2x40: FP64 113.0
+// -> 117.8 M steps/s, FP32 122.7 -> 141.2 M); one (255 registers, 8 warps) elsewhere, where
+// three or four measured slower (pumped lossy mode E = 1: -1 % / -12 %; interaction-picture
+// E = 3: -6 % / -14 %).
+template <int E, bool IP>
+struct WarpMinBlocks {
+  static constexpr int value = (!IP && E == 3) ? 3 : 1;
+};
 
 template <typename R, int E, int SMAX, bool IP>
-__global__ void __launch_bounds__(128, CQG_MIN_BLOCKS) mcwfWarpKernel(TrajDev td, RunArgs ra) {
+__global__ void __launch_bounds__(128, (WarpMinBlocks<E, IP>::value)) mcwfWarpKernel(TrajDev td, RunArgs ra) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
