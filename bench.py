@@ -129,6 +129,8 @@ def parse():
     ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the batched-vs-plain, accuracy and serving checks of the default line")
     ap.add_argument("--apply-states", type=int, default=0,
                     help="only time the batched H/i application on this many states of the workload's system")
     ap.add_argument("--apply-reps", type=int, default=20)
@@ -606,8 +608,146 @@ def run_serving(args, dev):
                     "d2h_bytes_per_step": None}}
 
 
+# Correctness check 2 of the bench's default line: the FP64 master equation of the qubit-mode
+# workload over t in [0, 20], computed by the oracle and committed as a fixture (a CPU test
+# recomputes it and requires the same numbers).
+MASTER_FIXTURE = os.path.join(ROOT, "tests", "golden", "master_equation_runs.json")
+
+
+def bonferroni_z(n_comparisons, sigmas=3.0):
+    """Per-point z threshold of a 3-sigma family-wise test over n_comparisons points."""
+    from scipy.stats import norm
+    return float(norm.isf(2 * norm.sf(sigmas) / (2 * n_comparisons)))
+
+
+def accuracy_summary(precision, n_traj=4096):
+    """Ensemble averages of the qubit-mode workload (t in [0, 20], Dt = 1, from the vacuum)
+    against the FP64 master equation: per output time and observable, the distance in units
+    of the ensemble's standard error (per-trajectory values)."""
+    import numpy as np
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    ref = json.load(open(MASTER_FIXTURE))["qbitmode_jc_2x40"]
+    model = cqg.Model(ref["script"], ref["args"])
+    pars = model.run_pars().mcwf
+    pars.precision = precision
+    ens = cqg.Ensemble(cqg.System(model.desc), model.initial_state(), n_traj, pars)
+    K = int(round(ref["T"] / ref["Dt"]))
+    master = np.array(ref["rows"])[1:, 2:]
+    z = np.zeros((K, 4))
+    for k in range(K):
+        ens.run(ref["Dt"], 1)
+        per = ens.traj_averages()[:, :model.n_avr]
+        # <n>, Re<a>, Im<a>, <sigma_z> = rho11 - rho00 (columns of the qubit-mode key)
+        obs = np.stack([per[:, 4], per[:, 6], per[:, 7], per[:, 1] - per[:, 0]], axis=1)
+        want = np.array([master[k, 4], master[k, 6], master[k, 7], master[k, 1] - master[k, 0]])
+        se = obs.std(axis=0, ddof=1) / np.sqrt(n_traj)
+        # an observable that is the same in every trajectory (Im<a> = 0 here) has no spread:
+        # floor the error by the integrators' accuracy
+        floor = 1e-6 if precision == A.FP64 else 1e-4
+        z[k] = np.abs(obs.mean(axis=0) - want) / np.sqrt(se ** 2 + floor ** 2)
+    return {"observables": ["<n>", "Re<a>", "Im<a>", "<sigma_z>"], "t": [ref["Dt"] * (k + 1) for k in range(K)],
+            "sigma": np.round(z, 3).tolist(), "max_sigma_per_observable": np.round(z.max(axis=0), 3).tolist(),
+            "max_sigma": float(z.max()), "bonferroni_3sigma_threshold": bonferroni_z(z.size),
+            "within_3sigma": bool(z.max() < bonferroni_z(z.size))}
+
+
+def uneven_summary(rng, steps=3, warmup=1):
+    """The uneven batch (256 driven Jaynes-Cummings systems, D in [40, 240], 64 trajectories
+    each): one batch in FP32-state and in FP64, against the plain path (one FP64 ensemble
+    per system and launch, one after another), over the same Dt intervals; device time of
+    the run calls.  Also the FP32 batch means against the FP64 batch (same streams)."""
+    import numpy as np
+    import torch
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    n_sys, per, Dt = UNEVEN["uneven_jc_16384"]
+    models = uneven_models(n_sys)
+    systems = [cqg.System(m.desc) for m in models]
+    idx = np.repeat(np.arange(n_sys), per)
+    psi0s = [models[j].initial_state() for j in idx]
+
+    def pars_for(precision, stream=1):
+        p = models[0].run_pars().mcwf
+        p.rng = A.RNG_PCG64 if rng == "pcg64" else A.RNG_PHILOX
+        p.precision = precision
+        p.prng_stream = stream
+        return p
+
+    def timed(ens):
+        for _ in range(warmup):
+            ens.run(Dt, 1)
+        c0 = ens.counters()[:, 0].astype(np.int64)
+        ms = 0.0
+        for _ in range(steps):
+            ens.run(Dt, 1)
+            ms += ens.last_ms()[1]
+        return int((ens.counters()[:, 0].astype(np.int64) - c0).sum()), ms
+
+    out = {}
+    means = {}
+    for name, prec in (("batched_fp32", A.FP32), ("batched_fp64", A.FP64)):
+        ens = cqg.Ensemble.batch(systems, idx, psi0s, pars_for(prec))
+        st, ms = timed(ens)
+        out[name] = st / (ms * 1e-3)
+        means[name] = ens.traj_averages()[:, :models[0].n_avr]
+        del ens
+    p_steps, p_ms = 0, 0.0
+    for j in range(n_sys):
+        e = cqg.Ensemble(systems[j], models[j].initial_state(), per, pars_for(A.FP64, 1 + j * per))
+        st, ms = timed(e)
+        p_steps += st
+        p_ms += ms
+        del e
+    torch.cuda.synchronize()
+    out["plain_fp64"] = p_steps / (p_ms * 1e-3)
+    out["batched_fp32_vs_plain_fp64"] = out["batched_fp32"] / out["plain_fp64"]
+    out["batched_fp64_vs_plain_fp64"] = out["batched_fp64"] / out["plain_fp64"]
+    out["fp32_vs_fp64_batched"] = out["batched_fp32"] / out["batched_fp64"]
+    a64, a32 = means["batched_fp64"], means["batched_fp32"]
+    se = a64.std(axis=0, ddof=1) / np.sqrt(len(a64))
+    z = np.abs(a32.mean(axis=0) - a64.mean(axis=0)) / np.where(se > 0, se, np.inf)
+    out["fp32_vs_fp64_batch_means_max_sigma"] = float(z.max())
+    out["config"] = {"systems": n_sys, "trajectories_per_system": per, "Dt": Dt, "warmup_intervals": warmup,
+                     "timed_intervals": steps, "unit": "trajectory-steps/s (device time of the run calls)"}
+    return out
+
+
+def north_star_checks(args, dev):
+    """Extra keys of the default line: batched and served throughput against the plain
+    one-ensemble-per-launch FP64 path, and the accuracy of the FP64 and FP32-state ensembles
+    against the FP64 master equation."""
+    from cppqed_b200 import _abi as A
+
+    out = {"uneven_batch": uneven_summary(args.rng)}
+    out["accuracy_vs_master_equation"] = {
+        "workload": "qbitmode_jc_2x40, 4096 trajectories, t in [0, 20], Dt = 1",
+        "reference": "FP64 master equation of the oracle (tests/golden/master_equation_runs.json)",
+        "fp64": accuracy_summary(A.FP64), "fp32_state": accuracy_summary(A.FP32)}
+    sargs = argparse.Namespace(**vars(args))
+    sargs.workload = "serving_poisson_200"
+    sargs.precision = "fp32"
+    srv = run_serving(sargs, dev)
+    out["serving"] = {"workload": sargs.workload, "precision": "fp32-state/fp64-control",
+                      "latency_ms": srv["latency_ms"], "served_wall_steps_per_s": srv["value"],
+                      "served_device_steps_per_s": srv["device_value"],
+                      "plain_fp64_device_steps_per_s": srv["plain_fp64"]["value"],
+                      "served_device_vs_plain_fp64": srv["served_device_vs_plain"],
+                      "requests": srv["config"]["requests"], "failed_requests": srv["failed_requests"]}
+    return out
+
+
 def cpu_sample(args, threads, seconds):
-    """Times the oracle (the reference's serial algorithm) on a bounded sample."""
+    """Times the oracle (the reference's serial algorithm: Ensemble::advance trajectory by
+    trajectory, the density-operator average at every Dt) on a sample of the workload's
+    trajectories over the same time window as the device arm: args.warmup untimed intervals
+    of Dt, then args.steps timed ones.  The sample (the first n of the trajectories, the same
+    random streams) is sized so that the timed part takes about `seconds` on `threads`
+    host threads."""
     import cppqed_b200 as cqg
     from tests.oracle_lib import Oracle
 
@@ -615,16 +755,29 @@ def cpu_sample(args, threads, seconds):
     model = cqg.Model(script, sargs)
     pars = model.run_pars().mcwf
     orc = Oracle()
-    # calibrate: a few trajectories over one Dt
-    n = max(threads, 4)
-    steps, secs, _ = orc.ensemble_bench(model, pars, n, Dt, 1, threads, 1)
-    per_traj = secs / n
-    n = max(threads, int(seconds / max(per_traj, 1e-6)))
-    n = min(n, n_traj)
-    steps, secs, _ = orc.ensemble_bench(model, pars, n, Dt, 1, threads, 1)
+    W, K = args.warmup, max(args.steps, 1)
+    # calibrate on a few trajectories: cost of one interval after the warm-up
+    probe = max(threads, 4)
+    _, secs, _ = orc.ensemble_bench(model, pars, probe, Dt, 1, threads, 1, warm_intervals=W)
+    per_traj_interval = secs * threads / probe
+    n = int(seconds * threads / (K * max(per_traj_interval, 1e-6)))
+    n = max(threads, min(n_traj, n - n % threads if n > threads else threads))
+    steps, secs, _ = orc.ensemble_bench(model, pars, n, Dt, K, threads, 1, warm_intervals=W)
     return {"value": steps / secs, "unit": "trajectory-steps/s", "cores": threads, "kind": "port",
-            "sample": "%d trajectories x Dt=%g of %s (of %d), serial Ensemble::advance + rho average per Dt" %
-                      (n, Dt, args.workload, n_traj), "steps": steps, "seconds": secs}
+            "sample": "trajectories 1..%d of the %d of %s (the same random streams) through the device arm's "
+                      "window t in [%g, %g]: %d untimed warm-up intervals, then %d timed intervals of Dt = %g; "
+                      "serial Ensemble::advance + rho average per Dt, trajectories split over %d host threads" %
+                      (n, n_traj, args.workload, W * Dt, (W + K) * Dt, W, K, Dt, threads),
+            "steps": steps, "seconds": secs, "n_sample": n}
+
+
+def workload_config(args, world):
+    """The bench line's config, the same for the device arm and the reference arm."""
+    script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+    return {"workload": args.workload, "script": script, "args": " ".join(sargs), "n_traj_per_gpu": n_traj,
+            "Dt_per_step": Dt, "t_window": [args.warmup * Dt, (args.warmup + args.steps) * Dt], "rng": args.rng,
+            "l2_flush": "not needed: states stay on chip; per-step HBM traffic is the state read/write",
+            "parallelism": "trajectory-sharded x%d" % world}
 
 
 def main():
@@ -638,22 +791,16 @@ def main():
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        res = []
-        for _ in range(args.warmup):
-            pass
-        for _ in range(args.steps):
-            res.append(cpu_sample(args, threads, max(1.0, args.cpu_sample_seconds / max(args.steps, 1))))
-        value = sum(r["steps"] for r in res) / sum(r["seconds"] for r in res)
-        script, sargs, n_traj, Dt = WORKLOADS[args.workload]
+        r = cpu_sample(args, threads, args.cpu_sample_seconds)
+        value = r["value"]
         out = {"metric": "MCWF trajectory-steps/s", "value": value, "unit": "trajectory-steps/s",
                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": 1e3 * sum(r["seconds"] for r in res) / len(res), "higher_is_better": True,
+               "ms_per_step": 1e3 * r["seconds"] / max(args.steps, 1), "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": args.workload, "script": script, "args": " ".join(sargs),
-                          "n_traj_per_gpu": n_traj, "Dt_per_step": Dt},
+               "config": workload_config(args, args.gpus),
                "impl": "reference",
                "cpu_baseline": {"value": value, "unit": "trajectory-steps/s", "cores": threads, "kind": "port",
-                                "sample": res[0]["sample"]},
+                                "sample": r["sample"]},
                "e2e": {"value": value, "unit": "trajectory-steps/s", "h2d_bytes_per_step": 0,
                        "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
@@ -681,16 +828,16 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(args, 1, args.cpu_sample_seconds)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and args.workload == "qbitmode_jc_2x40":
+        extras = north_star_checks(args, local)
     if rank == 0:
         script, sargs, n_traj, Dt = WORKLOADS[args.workload]
         out = {"metric": "MCWF trajectory-steps/s", "value": r["value"], "unit": "trajectory-steps/s",
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
-               "config": {"workload": args.workload, "script": script, "args": " ".join(sargs),
-                          "n_traj_per_gpu": n_traj, "Dt_per_step": Dt, "rng": args.rng,
-                          "l2_flush": "not needed: states stay on chip; per-step HBM traffic is the state read/write",
-                          "parallelism": "trajectory-sharded x%d" % world},
+               "config": workload_config(args, world),
                "e2e": r["e2e"], "roofline": r["roofline"], "apply_roofline": r["apply"], "cpu_baseline": cpu,
                "clocks": r["clocks"],
                "gpu_launches": 3 * args.steps,
@@ -698,6 +845,8 @@ def main():
                             "rhs_evaluations": r["rhs_total"], "failed_attempts": r["failed_total"],
                             "dp_limit_overshoots": r["overshoots_total"], "step_backs": r["stepbacks_total"],
                             "jumps": r["jumps_total"], "kernel_ms": r["kernel_ms"]}}
+        if extras is not None:
+            out["north_star"] = extras
         print(json.dumps(out))
     if world > 1:
         torch.distributed.barrier()

@@ -189,22 +189,6 @@ ENGINE_PROTOTYPES = {
     "cqg_model_destroy": (C.c_int, [_P]),
 }
 
-ORACLE_PROTOTYPES = {
-    "oracle_last_error": (C.c_char_p, []),
-    "oracle_pcg64_uniform": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int64, _DP]),
-    "oracle_pcg64_state_text": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int64, C.c_char_p, C.c_size_t]),
-    "oracle_apply_hamiltonian": (C.c_int, [C.POINTER(cqg_system_desc), _CP, C.c_double, _CP]),
-    "oracle_run": (C.c_int, [C.POINTER(cqg_system_desc), _CP, C.POINTER(cqg_run_pars), _DP, C.c_int64,
-                             C.POINTER(C.c_int64), _CP]),
-    "oracle_trajectory": (C.c_int, [C.POINTER(cqg_system_desc), _CP, C.POINTER(cqg_mcwf_pars), C.c_uint64,
-                                    C.c_double, C.c_int64, C.c_double, _CP, _DP, C.POINTER(C.c_uint64),
-                                    _DP, C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
-    "oracle_ensemble_bench": (C.c_int, [C.POINTER(cqg_system_desc), _CP, C.POINTER(cqg_mcwf_pars), C.c_int64,
-                                        C.c_double, C.c_int64, C.c_int32, C.c_int32,
-                                        C.POINTER(C.c_uint64), _DP, _DP]),
-}
-
-
 def bind(lib, prototypes):
     for name, (res, args) in prototypes.items():
         fn = getattr(lib, name)

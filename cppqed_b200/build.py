@@ -94,15 +94,7 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     return info
 
 
-def build_oracle(verbose=False):
-    """Builds the CPU oracle (test infrastructure) with its Makefile."""
-    out = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
-    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "PYTHON=" + sys.executable], verbose)
-    return out
-
-
 if __name__ == "__main__":
     txt = build(verbose=True, ptxas_info="--ptxas-info" in sys.argv)
     if txt:
         print(txt)
-    build_oracle(verbose=True)

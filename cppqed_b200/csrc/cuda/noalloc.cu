@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -37,20 +38,32 @@ static __device__ __align__(256) double gNoallocScratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
 std::mutex gSetupMutex;
-double* gScratchPtr[kMaxDevices] = {};
+// Per device: the array's device address and the SM count, resolved at the first call on the
+// device with that device current.  A cudaDeviceReset would reload the module and move the
+// array, so the library must not be used across a device reset.
+struct DeviceSetup {
+  double* scratch = nullptr;
+  int sms = 0;
+};
+DeviceSetup gSetup[kMaxDevices];
 
-// Resolves the device address of the scratch array for the current device (once per device).
-int scratchFor(int device, double** out) {
+int setupFor(int device, DeviceSetup* out) {
   if (device < 0 || device >= kMaxDevices) return fail(CQG_E_UNSUPPORTED, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(gSetupMutex);
-  if (!gScratchPtr[device]) {
+  DeviceSetup& d = gSetup[device];
+  if (!d.scratch) {
     void* p = nullptr;
-    const cudaError_t err = cudaGetSymbolAddress(&p, gNoallocScratch);
+    cudaError_t err = cudaGetSymbolAddress(&p, gNoallocScratch);
     if (err != cudaSuccess)
       return fail(CQG_E_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(err));
-    gScratchPtr[device] = static_cast<double*>(p);
+    int sms = 0;
+    err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (err != cudaSuccess || sms < 1)
+      return fail(CQG_E_CUDA, std::string("cudaDeviceGetAttribute(SM count): ") + cudaGetErrorString(err));
+    d.sms = sms;
+    d.scratch = static_cast<double*>(p);
   }
-  *out = gScratchPtr[device];
+  *out = d;
   return CQG_OK;
 }
 
@@ -70,10 +83,11 @@ __global__ void __launch_bounds__(128) stateAveragesKernel(SysDev sys, const dou
     for (int k = 0; k < sys.nObs; ++k) {
       const double2* ov = sys.oval + size_t(k) * sys.SO * D;
       const int* oc = sys.ocol + size_t(k) * sys.SO * D;
+      const int nSk = sys.oS[k];  // this observable's slots; the rest of SO is zero padding
       double re = 0., im = 0.;
       for (int r = lane; r < D; r += 32) {
         double2 acc = make_double2(0., 0.);
-        for (int s = 0; s < sys.SO; ++s) acc = cqg::dev::cfma(ov[s * D + r], x[oc[s * D + r]], acc);
+        for (int s = 0; s < nSk; ++s) acc = cqg::dev::cfma(ov[s * D + r], x[oc[s * D + r]], acc);
         const double2 xr = x[r];
         re += xr.x * acc.x + xr.y * acc.y;  // conj(psi_r) (O psi)_r
         im += xr.x * acc.y - xr.y * acc.x;
@@ -111,6 +125,11 @@ extern "C" int cqg_system_averages_noalloc(const cqg_system* sys, const cqg_comp
                                            double* sums, void* stream) {
   if (!sys || !psi || !sums || n_states < 1)
     return fail(CQG_E_INVALID, "cqg_system_averages_noalloc: null pointer or no states");
+  // the kernel reads states as 16-byte complex vectors and writes doubles
+  if (reinterpret_cast<uintptr_t>(psi) % 16 != 0)
+    return fail(CQG_E_INVALID, "cqg_system_averages_noalloc: psi must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(sums) % 8 != 0)
+    return fail(CQG_E_INVALID, "cqg_system_averages_noalloc: sums must be 8-byte aligned");
   const SysDev* sd = cqg::dev::systemDescriptor(sys);
   const int nAvr = sd->nAvr;
   if (nAvr < 1) return fail(CQG_E_INVALID, "cqg_system_averages_noalloc: the system has no averages");
@@ -122,11 +141,12 @@ extern "C" int cqg_system_averages_noalloc(const cqg_system* sys, const cqg_comp
   if (err != cudaSuccess) return fail(CQG_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(err));
   if (device != cqg::dev::systemDevice(sys))
     return fail(CQG_E_INVALID, "cqg_system_averages_noalloc: the current device is not the system's device");
-  double* slots = nullptr;
-  if (int rc = scratchFor(device, &slots)) return rc;
+  DeviceSetup setup;
+  if (int rc = setupFor(device, &setup)) return rc;
+  double* slots = setup.scratch;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const long long warpsWanted = n_states;
-  const int blocks = int(std::min<long long>((warpsWanted + 3) / 4, 148ll * 16));
+  // one warp per state, four per CTA, at most 16 CTAs per SM (grid-stride beyond that)
+  const int blocks = int(std::min<long long>((n_states + 3) / 4, 16ll * setup.sms));
   stateAveragesKernel<<<blocks, 128, 0, s>>>(*sd, reinterpret_cast<const double2*>(psi), n_states, nAvr, slots);
   err = cudaGetLastError();
   if (err != cudaSuccess) return fail(CQG_E_CUDA, std::string("state averages launch: ") + cudaGetErrorString(err));

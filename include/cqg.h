@@ -352,11 +352,16 @@ int cqg_ensemble_destroy(cqg_ensemble* ens);
  * synchronise the device.  Allocates nothing: the per-state intermediate sums live in
  * one fixed device array of 2^18 doubles held by every GPU that loads the library, so
  * n_states * n_avr must not exceed 262144 (larger requests fail with CQG_E_INVALID).
- * psi and sums are device pointers; work is queued on `stream` (a cudaStream_t, NULL
- * for the default stream) and the call returns without waiting.  The first call on a
- * device looks up the array's device address, so make that first call before any
- * stream capture.  All calls share the array: calls whose work overlaps on the GPU
- * race and give wrong sums.  The current device must be the system's device. */
+ * The states are used as given: they are not renormalised, and for systems with an
+ * interaction picture they must already be in the frame of the output time (t0 = t, as
+ * the ensemble path has them at its output times).  psi (16-byte aligned) and sums
+ * (8-byte aligned) are device pointers; misaligned pointers fail with CQG_E_INVALID
+ * before any work is queued.  Work is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without waiting.  The first call on a device
+ * looks up the array's device address and the device's SM count, so make that first call
+ * before any stream capture, and do not use the library across a cudaDeviceReset.  All
+ * calls share the array: calls whose work overlaps on the GPU race and give wrong sums.
+ * The current device must be the system's device. */
 int cqg_system_averages_noalloc(const cqg_system* sys, const cqg_complex* psi, int64_t n_states, double* sums,
                                 void* stream);
 

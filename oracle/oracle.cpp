@@ -34,6 +34,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <memory>
 #include <thread>
 #include <vector>
 
@@ -952,43 +953,61 @@ int oracle_trajectory(const cqg_system_desc* d, const cqg_complex* psi0c, const 
 // thread with its own system copy (the reference's caches are not thread-safe).
 // Returns accepted MCWF steps and wall seconds.
 int oracle_ensemble_bench(const cqg_system_desc* d, const cqg_complex* psi0c, const cqg_mcwf_pars* p, int64_t n_traj,
-                          double Dt, int64_t n_intervals, int32_t threads, int32_t with_rho, uint64_t* steps_out,
-                          double* seconds_out, double* avr_sum_out) {
+                          double Dt, int64_t warm_intervals, int64_t n_intervals, int32_t threads, int32_t with_rho,
+                          uint64_t* steps_out, double* seconds_out, double* avr_sum_out) {
+  // The serial Ensemble::advance of the reference (StochasticTrajectory.h:220-245) with the
+  // density-operator average at every Dt (MCWF_Trajectory.h:406-420), its trajectories split
+  // over `threads` workers: warm_intervals untimed intervals first (the same time window as a
+  // device run that starts after its warm-up), then n_intervals timed ones.  Steps and seconds
+  // are those of the timed intervals.
   try {
     if (threads < 1) threads = 1;
+    if (warm_intervals < 0 || n_intervals < 0) throw std::invalid_argument("negative interval count");
     const System proto(*d);
     CVec psi0(proto.D);
     for (size_t i = 0; i < proto.D; ++i) psi0[i] = C(psi0c[i]);
+    std::vector<std::unique_ptr<System>> systems;
+    std::vector<std::vector<Trajectory>> trs(threads);
+    for (int w = 0; w < threads; ++w) systems.emplace_back(new System(*d));
     std::vector<uint64_t> steps(threads, 0);
     std::vector<std::vector<double>> avrs(threads, std::vector<double>(proto.nAvr * n_intervals, 0.));
     std::vector<std::string> errs(threads);
-    auto t0 = std::chrono::steady_clock::now();
-    std::vector<std::thread> pool;
-    for (int w = 0; w < threads; ++w)
-      pool.emplace_back([&, w] {
-        try {
-          System s(*d);
-          std::vector<Trajectory> trs;
-          for (int64_t i = w; i < n_traj; i += threads) trs.emplace_back(&s, psi0, *p, p->prng_stream + i);
-          CVec rho;
-          std::vector<double> avr(s.nAvr);
-          for (int64_t k = 0; k < n_intervals; ++k) {
-            for (auto& tr : trs) tr.advance(Dt);
-            if (with_rho && !trs.empty()) {
-              ensembleRho(trs, s.D, rho);
-              averagesRho(s, rho, avr.data());
-              for (int c = 0; c < s.nAvr; ++c) avrs[w][k * s.nAvr + c] = avr[c] * double(trs.size());
+    auto phase = [&](int64_t first, int64_t count, bool timed) {
+      std::vector<std::thread> pool;
+      for (int w = 0; w < threads; ++w)
+        pool.emplace_back([&, w] {
+          try {
+            System& s = *systems[w];
+            if (trs[w].empty())
+              for (int64_t i = w; i < n_traj; i += threads) trs[w].emplace_back(&s, psi0, *p, p->prng_stream + i);
+            size_t before = 0;
+            for (auto& tr : trs[w]) before += tr.nSteps;
+            CVec rho;
+            std::vector<double> avr(s.nAvr);
+            for (int64_t k = first; k < first + count; ++k) {
+              for (auto& tr : trs[w]) tr.advance(Dt);
+              if (with_rho && !trs[w].empty()) {
+                ensembleRho(trs[w], s.D, rho);
+                averagesRho(s, rho, avr.data());
+                if (timed)
+                  for (int c = 0; c < s.nAvr; ++c) avrs[w][k * s.nAvr + c] = avr[c] * double(trs[w].size());
+              }
             }
+            size_t after = 0;
+            for (auto& tr : trs[w]) after += tr.nSteps;
+            if (timed) steps[w] = after - before;
+          } catch (const std::exception& e) {
+            errs[w] = e.what();
           }
-          for (auto& tr : trs) steps[w] += tr.nSteps;
-        } catch (const std::exception& e) {
-          errs[w] = e.what();
-        }
-      });
-    for (auto& th : pool) th.join();
+        });
+      for (auto& th : pool) th.join();
+      for (auto& e : errs)
+        if (!e.empty()) throw std::runtime_error(e);
+    };
+    phase(0, warm_intervals, false);
+    auto t0 = std::chrono::steady_clock::now();
+    phase(0, n_intervals, true);
     auto t1 = std::chrono::steady_clock::now();
-    for (auto& e : errs)
-      if (!e.empty()) throw std::runtime_error(e);
     uint64_t total = 0;
     for (auto s : steps) total += s;
     *steps_out = total;

@@ -17,8 +17,9 @@ def _ensure_built():
     from cppqed_b200 import build
     if not os.path.exists(build.LIB):
         build.build()
-    if not os.path.exists(os.path.join(ROOT, "oracle", "_build", "liboracle.so")):
-        build.build_oracle()
+    from tests import oracle_lib
+    if not os.path.exists(oracle_lib.PATH):
+        oracle_lib.build_oracle()
 
 
 @pytest.fixture(scope="session")

@@ -4,6 +4,8 @@ The oracle is the checker: a restatement of the reference's MCWF path that the
 device results are compared with.  Nothing in the engine imports this module."""
 import ctypes as C
 import os
+import subprocess
+import sys
 
 import numpy as np
 
@@ -12,10 +14,41 @@ from cppqed_b200 import _abi as A
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PATH = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 
+_CP = C.POINTER(A.cqg_complex)
+_DP = C.POINTER(C.c_double)
+
+# C prototypes of the oracle library (oracle/oracle.cpp)
+ORACLE_PROTOTYPES = {
+    "oracle_last_error": (C.c_char_p, []),
+    "oracle_pcg64_uniform": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int64, _DP]),
+    "oracle_pcg64_state_text": (C.c_int, [C.c_uint64, C.c_uint64, C.c_int64, C.c_char_p, C.c_size_t]),
+    "oracle_apply_hamiltonian": (C.c_int, [C.POINTER(A.cqg_system_desc), _CP, C.c_double, _CP]),
+    "oracle_run": (C.c_int, [C.POINTER(A.cqg_system_desc), _CP, C.POINTER(A.cqg_run_pars), _DP, C.c_int64,
+                             C.POINTER(C.c_int64), _CP]),
+    "oracle_trajectory": (C.c_int, [C.POINTER(A.cqg_system_desc), _CP, C.POINTER(A.cqg_mcwf_pars), C.c_uint64,
+                                    C.c_double, C.c_int64, C.c_double, _CP, _DP, C.POINTER(C.c_uint64),
+                                    _DP, C.POINTER(C.c_int32), C.c_int64, C.POINTER(C.c_int64)]),
+    "oracle_ensemble_bench": (C.c_int, [C.POINTER(A.cqg_system_desc), _CP, C.POINTER(A.cqg_mcwf_pars), C.c_int64,
+                                        C.c_double, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                        C.POINTER(C.c_uint64), _DP, _DP]),
+}
+
+
+def build_oracle(verbose=False):
+    """Builds the CPU oracle with its Makefile (oracle/_build/liboracle.so)."""
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), "PYTHON=" + sys.executable]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("oracle build failed")
+    return PATH
+
 
 class Oracle:
     def __init__(self):
-        self.lib = A.bind(C.CDLL(PATH), A.ORACLE_PROTOTYPES)
+        self.lib = A.bind(C.CDLL(PATH), ORACLE_PROTOTYPES)
 
     def _err(self):
         return self.lib.oracle_last_error().decode()
@@ -83,14 +116,18 @@ class Oracle:
         self.lib.oracle_pcg64_state_text(seed, stream, n_draws, buf, 256)
         return buf.value.decode()
 
-    def ensemble_bench(self, model, pars, n_traj, Dt, n_intervals, threads=1, with_rho=True):
+    def ensemble_bench(self, model, pars, n_traj, Dt, n_intervals, threads=1, with_rho=True, warm_intervals=0):
+        """The reference's serial ensemble on n_traj trajectories: warm_intervals untimed
+        intervals of Dt, then n_intervals timed ones.  (steps, seconds, sums per interval) of
+        the timed part."""
         steps = C.c_uint64()
         secs = C.c_double()
         sums = np.zeros(n_intervals * model.n_avr)
         psi = model.initial_state()
         rc = self.lib.oracle_ensemble_bench(model.desc, psi.ctypes.data_as(C.POINTER(A.cqg_complex)), C.byref(pars),
-                                            int(n_traj), float(Dt), int(n_intervals), int(threads), int(with_rho),
-                                            C.byref(steps), C.byref(secs), sums.ctypes.data_as(C.POINTER(C.c_double)))
+                                            int(n_traj), float(Dt), int(warm_intervals), int(n_intervals),
+                                            int(threads), int(with_rho), C.byref(steps), C.byref(secs),
+                                            sums.ctypes.data_as(C.POINTER(C.c_double)))
         if rc:
             raise RuntimeError(self._err())
         return steps.value, secs.value, sums.reshape(n_intervals, model.n_avr)

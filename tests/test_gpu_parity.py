@@ -106,70 +106,101 @@ def _master_rows(oracle, model, T, Dt):
     return oracle.run(model, rp)
 
 
+def bonferroni_z(n_comparisons, sigmas=3.0):
+    """Per-comparison z threshold that keeps the family-wise two-sided error of a 3-sigma
+    test (0.27 %) over n_comparisons points (Bonferroni)."""
+    from scipy.stats import norm
+    return float(norm.isf(2 * norm.sf(sigmas) / (2 * n_comparisons)))
+
+
+def interval_statistics(ens, Dt, K, n_avr):
+    """K output intervals of Dt: per interval the ensemble mean and the standard error of
+    every linear average column, from the per-trajectory values."""
+    means, errs = [], []
+    for _ in range(K):
+        ens.run(Dt, 1)
+        per = ens.traj_averages()[:, :n_avr]
+        means.append(per.mean(axis=0))
+        errs.append(per.std(axis=0, ddof=1) / np.sqrt(len(per)))
+    return np.array(means), np.array(errs)
+
+
+def z_scores(mean, err, ref, floor):
+    """|mean - ref| in units of the standard error, the error floored by the integrators'
+    numerical accuracy (an observable that is the same in every trajectory has no spread)."""
+    return np.abs(mean - ref) / np.sqrt(err ** 2 + floor ** 2)
+
+
+# Numerical floor of the comparisons: the controlled Cash-Karp at eps 1e-6 keeps a
+# trajectory's averages within ~3e-8 of the analytic coherent state of the pumped lossy mode
+# over t in [0, 10] (measured on the oracle), and the master equation within 5e-9; FP32
+# states add rounding of ~1e-7 per step.
+FLOOR_FP64 = 1e-6
+FLOOR_FP32 = 1e-4
+
+
 @pytest.mark.parametrize("rng", [A.RNG_PHILOX, A.RNG_PCG64])
 def test_pumped_lossy_mode_ensemble_vs_master(gpu, oracle, rng):
+    """Correctness check 2 on the pumped lossy mode (D = 30, 1000 trajectories, t in [0, 10]):
+    <n>, Re<a>, Im<a> of the ensemble agree with the master equation within 3 sigma
+    (Bonferroni over every output time and observable), and with the analytic coherent state
+    <a>(t) = alpha_ss (1 - exp((-kappa + i Delta) t)), alpha_ss = eta / (kappa - i Delta)
+    (PumpedLossyMode_Evolved.cc:31-33), <n> = |<a>|^2, to the integrators' accuracy."""
     model = gpu.Model("PumpedLossyMode_C++QED", C1_ARGS)
-    n = 2048
+    n = 1000
     pars = model.run_pars().mcwf
     pars.rng = rng
     sysd = gpu.System(model.desc)
     ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
-    Dt, K = 0.5, 8
-    sums = ens.run(Dt, K)
-    per = ens.traj_averages()  # last run's first interval only; use sums for means
+    Dt, K = 0.5, 20
+    mean, err = interval_statistics(ens, Dt, K, model.n_avr)
     master = _master_rows(oracle, model, Dt * K, Dt)
-    # columns: <n>, VAR(n) (processed), Re<a>, Im<a>
-    mean = sums[:, :model.n_avr] / n
-    for k in range(K):
-        ref = master[k + 1, 2:]
-        m_n, m_re, m_im = mean[k, 0], mean[k, 2], mean[k, 3]
-        # a coherent state stays coherent through jumps: Var(<a>) across trajectories is tiny,
-        # Var(n) per trajectory is <n>; allow 3 sigma + 1% model margin
-        sig_n = np.sqrt(max(ref[0], 1e-3) / n) * 3 + 0.01 * ref[0]
-        assert abs(m_n - ref[0]) <= sig_n
-        assert abs(m_re - ref[2]) <= 0.02 + 0.01 * abs(ref[2])
-        assert abs(m_im - ref[3]) <= 0.02 + 0.01 * abs(ref[3])
+    # linear columns: <n>, <n^2>, Re<a>, Im<a>; processed master columns: <n>, VAR(n), Re<a>, Im<a>
+    cols = [0, 2, 3]
+    ref = master[1:, 2:][:, cols]
+    z = z_scores(mean[:, cols], err[:, cols], ref, FLOOR_FP64)
+    assert z.max() < bonferroni_z(z.size), z.max()
+    t = Dt * np.arange(1, K + 1)
+    delta, eta, kappa = -1.0, 2.0, 1.0
+    alpha = eta / (kappa - 1j * delta) * (1 - np.exp((-kappa + 1j * delta) * t))
+    assert np.abs(mean[:, 2] + 1j * mean[:, 3] - alpha).max() < FLOOR_FP64
+    assert np.abs(mean[:, 0] - np.abs(alpha) ** 2).max() < FLOOR_FP64
 
 
-def test_qbit_mode_ensemble_vs_master(gpu, oracle):
+def _qbit_mode_check(gpu, oracle, precision, floor):
     model = gpu.Model("QbitMode_C++QED", C2_ARGS)
     n = 4096
     pars = model.run_pars().mcwf
     pars.rng = A.RNG_PHILOX
+    pars.precision = precision
     sysd = gpu.System(model.desc)
     ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
-    Dt, K = 0.25, 8
-    sums = ens.run(Dt, K)
-    master = _master_rows(oracle, model, Dt * K, Dt)
-    per_last = None
-    mean = sums[:, :model.n_avr] / n
-    # columns: rho00, rho11, Re rho10, Im rho10, <n>, VAR(n), Re<a>, Im<a>
-    z = []
-    for k in range(K):
-        ref = master[k + 1, 2:]
-        p11 = ref[1]
-        sig_rho11 = np.sqrt(max(p11 * (1 - p11), 1e-4) / n)
-        z.append(abs(mean[k, 1] - p11) / sig_rho11)
-        sig_n = np.sqrt(max(ref[5] + ref[4], 1e-2) / n)
-        z.append(abs(mean[k, 4] - ref[4]) / sig_n)
-    z = np.array(z)
-    assert z.max() < 4.0, z  # 3 sigma with a Bonferroni margin for 16 comparisons
+    Dt, K = 1.0, 20
+    mean, err = interval_statistics(ens, Dt, K, model.n_avr)
+    master = _master_rows(oracle, model, Dt * K, Dt)[1:, 2:]
+    # linear columns: rho00, rho11, Re rho10, Im rho10, <n>, <n^2>, Re<a>, Im<a>
+    # <sigma_z> = rho11 - rho00 = 2 rho11 - 1 per (normalised) trajectory
+    per_sz_err = 2 * err[:, 1]
+    got = np.stack([mean[:, 4], mean[:, 6], mean[:, 7], mean[:, 1] - mean[:, 0]], axis=1)
+    se = np.stack([err[:, 4], err[:, 6], err[:, 7], per_sz_err], axis=1)
+    ref = np.stack([master[:, 4], master[:, 6], master[:, 7], master[:, 1] - master[:, 0]], axis=1)
+    z = z_scores(got, se, ref, floor)
+    return z
 
 
-def test_fp32_state_error_vs_fp64(gpu):
-    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
-    sysd = gpu.System(model.desc)
-    res = {}
-    for prec in (A.FP64, A.FP32):
-        pars = model.run_pars().mcwf
-        pars.rng = A.RNG_PHILOX
-        pars.precision = prec
-        ens = gpu.Ensemble(sysd, model.initial_state(), 4096, pars)
-        res[prec] = ens.run(0.25, 8)[:, :model.n_avr] / 4096
-    diff = np.abs(res[A.FP32] - res[A.FP64])
-    # same random streams; FP32 state flips few jump decisions: averages agree to ~3 sigma
-    assert diff[:, 4].max() < 0.1
-    assert diff[:, 1].max() < 0.05
+def test_qbit_mode_ensemble_vs_master(gpu, oracle):
+    """Correctness check 2 on the qubit-mode Jaynes-Cummings system (2 x 40, 4096
+    trajectories, t in [0, 20]): <n>, Re<a>, Im<a> and <sigma_z> agree with the master
+    equation within 3 sigma, Bonferroni over the 80 compared points."""
+    z = _qbit_mode_check(gpu, oracle, A.FP64, FLOOR_FP64)
+    assert z.max() < bonferroni_z(z.size), z
+
+
+def test_fp32_state_ensemble_vs_master(gpu, oracle):
+    """The FP32-state / FP64-control variant passes the same check 2 against the FP64 master
+    equation (the error of every observable is stated in sigma units by the bench)."""
+    z = _qbit_mode_check(gpu, oracle, A.FP32, FLOOR_FP32)
+    assert z.max() < bonferroni_z(z.size), z
 
 
 def test_stalled_trajectory_reports_status(gpu):
@@ -266,6 +297,7 @@ def test_uneven_batch_matches_each_trajectory_alone(gpu):
     pars = models[0].run_pars().mcwf
     batch = gpu.Ensemble.batch(systems, idx, psi0s, pars)
     batch.run(0.25, 2)
+    agree = 0
     for i, j in enumerate(order):
         p = models[j].run_pars().mcwf
         p.prng_stream = pars.prng_stream + i
@@ -273,10 +305,13 @@ def test_uneven_batch_matches_each_trajectory_alone(gpu):
         alone.run(0.25, 2)
         a = alone.state(0, models[j].dim)
         b = batch.state(i, models[j].dim)
-        ja, _ = alone.jumps(0)
-        jb, _ = batch.jumps(i)
-        if len(ja) == len(jb) and np.allclose(ja, jb, rtol=1e-9):
+        ja, la = alone.jumps(0)
+        jb, lb = batch.jumps(i)
+        if len(ja) == len(jb) and np.allclose(ja, jb, rtol=1e-9) and np.array_equal(la, lb):
+            agree += 1
             assert np.linalg.norm(a - b) < 1e-8, (i, j)
+    # a marginal jump decision may flip on rounding; every other trajectory must replay
+    assert agree >= len(order) - 1, agree
 
 
 # ---- batched H/i application (Tridiagonal::apply / Hamiltonian::addContribution) ----

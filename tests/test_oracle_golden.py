@@ -49,3 +49,28 @@ def test_uniform_draws_are_canonical(oracle):
     u = oracle.pcg64_uniform(1001, 1, 10000)
     assert u.min() >= 0 and u.max() < 1
     assert abs(u.mean() - 0.5) < 0.02
+
+
+def test_master_equation_fixture_is_the_oracle(oracle):
+    """The bench states the error of the ensemble averages against the FP64 master equation
+    held in tests/golden/master_equation_runs.json; it must be what the oracle computes."""
+    import json
+    import os
+
+    import cppqed_b200 as cqg
+    from cppqed_b200 import _abi as A
+
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "master_equation_runs.json")
+    runs = json.load(open(path))
+    assert runs
+    for name, r in runs.items():
+        model = cqg.Model(r["script"], r["args"])
+        rp = model.run_pars()
+        rp.evol = A.EVOL_MASTER
+        rp.dc = 0
+        rp.T = r["T"]
+        rp.Dt = r["Dt"]
+        rp.NDt = 0
+        rows = oracle.run(model, rp)
+        assert model.key() == r["key"], name
+        assert np.allclose(rows, np.array(r["rows"]), rtol=1e-13, atol=1e-15), name
