@@ -153,6 +153,9 @@ ENGINE_PROTOTYPES = {
     "cqg_ensemble_get_logger_maxima": (C.c_int, [_P, _DP, _DP, _DP]),
     "cqg_ensemble_get_jumps": (C.c_int, [_P, C.c_int64, C.c_int32, _DP, C.POINTER(C.c_int32),
                                          C.POINTER(C.c_int32)]),
+    "cqg_ensemble_get_jump_rings": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_uint64), _DP,
+                                              C.POINTER(C.c_int32)]),
+    "cqg_ensemble_set_jump_capacity": (C.c_int, [_P, C.c_int32]),
     "cqg_ensemble_status": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "cqg_ensemble_last_kernel_ms": (C.c_int, [_P, _DP, _DP]),
     "cqg_ensemble_save": (C.c_int, [_P, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
@@ -186,6 +189,9 @@ ENGINE_PROTOTYPES = {
     "cqg_model_n_avr": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "cqg_model_process": (C.c_int, [_P, _DP]),
     "cqg_model_key": (C.c_int, [_P, C.c_char_p, C.c_size_t]),
+    "cqg_model_key_text": (C.c_int, [_P, C.c_int32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "cqg_model_parameters_text": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "cqg_model_command_line": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "cqg_model_destroy": (C.c_int, [_P]),
 }
 

@@ -21,8 +21,12 @@ HOST_SOURCES = ["host/tridiagonal.cpp", "host/elements.cpp", "host/model.cpp", "
 CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu", "cuda/kernels_block.cu", "cuda/apply.cu", "cuda/server.cu", "cuda/master.cu"]
 # the kernel instantiations: one object per (precision, rows per lane)
 KERNEL_INSTANCES = [(r, e) for r in ("double", "float") for e in (1, 2, 3, 4)]
-HEADERS = ["cuda/engine_internal.cuh", "cuda/kernels_inst.cu", "cuda/mcwf_kernel.cuh", "cuda/mcwf_block.cuh", "cuda/rng.cuh", "host/lowering.hpp", "host/errors.hpp", "host/model.hpp",
-           "host/elements.hpp", "host/tridiagonal.hpp", "host/pars.hpp"]
+# what each kind of object is rebuilt for (besides its own source and include/*.h)
+HOST_HEADERS = ["host/lowering.hpp", "host/errors.hpp", "host/model.hpp", "host/elements.hpp", "host/tridiagonal.hpp",
+                "host/pars.hpp"]
+KERNEL_HEADERS = ["cuda/mcwf_kernel.cuh", "cuda/rng.cuh"]
+CUDA_HEADERS = ["cuda/engine_internal.cuh", "cuda/mcwf_kernel.cuh", "cuda/mcwf_block.cuh", "cuda/rng.cuh",
+                "host/lowering.hpp", "host/errors.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -52,13 +56,16 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     inc = ["-I" + os.path.join(ROOT, "include")]
-    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
-                                                          for h in ("cqg.h", "cqg_model.h")]
+    public = [os.path.join(ROOT, "include", h) for h in ("cqg.h", "cqg_model.h")]
+
+    def deps(names):
+        return [os.path.join(CSRC, h) for h in names] + public
+
     objs = []
     for src in HOST_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
-        if _stale(o, [s] + headers):
+        if _stale(o, [s] + deps(HOST_HEADERS)):
             _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", *inc, "-c", s, "-o", o], verbose)
         objs.append(o)
     info = ""
@@ -66,15 +73,15 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     for src in CUDA_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
-        jobs.append((s, o, []))
+        jobs.append((s, o, [], deps(CUDA_HEADERS)))
     inst = os.path.join(CSRC, "cuda", "kernels_inst.cu")
     for r, e in KERNEL_INSTANCES:
         jobs.append((inst, os.path.join(OBJDIR, "kernels_%s_e%d.o" % (r, e)),
-                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e]))
+                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e], deps(KERNEL_HEADERS)))
     procs = []
-    for s, o, defs in jobs:
+    for s, o, defs, hdrs in jobs:
         objs.append(o)
-        if _stale(o, [s] + headers) or ptxas_info:
+        if _stale(o, [s] + hdrs) or ptxas_info:
             cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs,
                    *extra_flags, "-c", s, "-o", o]
             if ptxas_info:
@@ -91,7 +98,25 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     out = lib or LIB
     if _stale(out, objs):
         _run([_nvcc(), *ARCH, "-shared", "-o", out, *objs, "-lcudart"], verbose)
+    if lib is None:
+        build_apps(verbose)
     return info
+
+
+APPS = {"cqg_evolve": "apps/cqg_evolve.cpp"}
+
+
+def build_apps(verbose=False):
+    """The C++ programs over the C ABI (include/cqg_ensemble.hpp), linked against libcqg.so
+    in the same directory."""
+    inc = os.path.join(ROOT, "include")
+    for name, src in APPS.items():
+        s = os.path.join(CSRC, src)
+        exe = os.path.join(LIBDIR, name)
+        deps = [s, LIB] + [os.path.join(inc, h) for h in ("cqg.h", "cqg_model.h", "cqg_ensemble.hpp")]
+        if _stale(exe, deps):
+            _run(["g++", "-std=c++17", "-O2", "-Wall", "-I" + inc, s, "-L" + LIBDIR, "-lcqg",
+                  "-Wl,-rpath,$ORIGIN", "-o", exe], verbose)
 
 
 if __name__ == "__main__":

@@ -94,6 +94,8 @@ struct cqg_ensemble {
   double* dSums = nullptr;
   size_t sumsCap = 0;
   int jumpCap = 64;
+  void* dJumpRing = nullptr;  // jump rings of a grown capacity (cqg_ensemble_set_jump_capacity)
+  size_t jumpRingBytes = 0;
   ~cqg_ensemble() {
     // nothing of this ensemble may still run on the blocks that go back to the cache
     int cur = 0;
@@ -110,6 +112,7 @@ struct cqg_ensemble {
     cqg::engine::deviceRelease(device, dAvr, avrCap * sizeof(double));
     cqg::engine::deviceRelease(device, dSums, sumsCap * sizeof(double));
     cqg::engine::deviceRelease(device, dmem, dmemBytes);
+    cqg::engine::deviceRelease(device, dJumpRing, jumpRingBytes);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evRun0) cudaEventDestroy(evRun0);
@@ -328,6 +331,49 @@ void buildSystemDevice(cqg_system& s) {
       fIdx[i] = static_cast<unsigned short>(it->second);
     }
   }
+  // The warp kernel's padded copies of the hot tables (see SysDev::wcol): rows to
+  // Dp = 32 ceil(D / 32), slots to kWarpSlots, zero coefficients on the row itself.
+  const bool warpTables = D <= kWarpKernelMaxD && S <= dev::kWarpSlots;
+  const int64_t Dp = (D + 31) / 32 * 32, WS = dev::kWarpSlots;
+  std::vector<int> wcol;
+  std::vector<dcomp> wdiag, wval, wlambda, wfreq;
+  std::vector<double> wjw;
+  std::vector<unsigned short> wfIdx;
+  if (warpTables) {
+    wcol.resize(size_t(WS * Dp));
+    wval.assign(size_t(WS * Dp), dcomp(0, 0));
+    wdiag.assign(size_t(Dp), dcomp(0, 0));
+    wjw.assign(size_t(nJ) * size_t(Dp), 0.);
+    for (int64_t r = 0; r < Dp; ++r) {
+      if (r < D) wdiag[r] = H.diag[r];
+      for (int64_t k = 0; k < WS; ++k) {
+        const bool real = r < D && k < S;
+        wcol[k * Dp + r] = real ? H.col[k * D + r] : int(r);
+        if (real) wval[k * Dp + r] = H.val[k * D + r];
+      }
+    }
+    for (int m = 0; m < nJ; ++m)
+      for (int64_t r = 0; r < D; ++r) wjw[size_t(m) * Dp + r] = jw[size_t(m) * D + r];
+    if (!L.lambda.empty()) {
+      wlambda.assign(size_t(Dp), dcomp(0, 0));
+      for (int64_t r = 0; r < D; ++r) wlambda[r] = L.lambda[r];
+    }
+    if (!H.freq.empty()) {
+      wfreq.assign(size_t(WS * Dp), dcomp(0, 0));
+      for (int64_t k = 0; k < S; ++k)
+        for (int64_t r = 0; r < D; ++r) wfreq[k * Dp + r] = H.freq[k * D + r];
+    }
+    if (!fIdx.empty()) {
+      wfIdx.assign(size_t(WS * Dp), dev::kNoPhase);
+      for (int64_t k = 0; k < S; ++k)
+        for (int64_t r = 0; r < D; ++r) wfIdx[k * Dp + r] = fIdx[k * D + r];
+    }
+  }
+  const size_t oWcol = A.add(wcol.size() * 4 + 4), oWdiagD = A.add(wdiag.size() * 16 + 16),
+               oWvalD = A.add(wval.size() * 16 + 16), oWdiagF = A.add(wdiag.size() * 8 + 8),
+               oWvalF = A.add(wval.size() * 8 + 8), oWjw = A.add(wjw.size() * 8 + 8),
+               oWlambda = A.add(wlambda.size() * 16 + 16), oWfIdx = A.add(wfIdx.size() * 2 + 16),
+               oWfreq = A.add(wfreq.size() * 16 + 16);
   const size_t oCol = A.add(H.col.size() * 4 + 4), oJcol = A.add(jcol.size() * 4 + 4), oJw = A.add(jw.size() * 8 + 8),
                oJHasW = A.add(jHasW.size() * 4 + 4), oOcol = A.add(ocol.size() * 4 + 4),
                oOval = A.add(oval.size() * 16 + 16), oORe = A.add(oRe.size() * 4 + 4), oOIm = A.add(oIm.size() * 4 + 4), oOS = A.add(oS.size() * 4 + 4),
@@ -360,6 +406,15 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oDiagF, toF2(H.diag));
   upload(b, oValF, toF2(H.val));
   upload(b, oJvalF, toF2(jval));
+  upload(b, oWcol, wcol);
+  upload(b, oWdiagD, toD2(wdiag));
+  upload(b, oWvalD, toD2(wval));
+  upload(b, oWdiagF, toF2(wdiag));
+  upload(b, oWvalF, toF2(wval));
+  upload(b, oWjw, wjw);
+  upload(b, oWlambda, toD2(wlambda));
+  upload(b, oWfIdx, wfIdx);
+  upload(b, oWfreq, toD2(wfreq));
   auto& sd = s.sd;
   sd.D = int(D);
   sd.S = S;
@@ -399,6 +454,16 @@ void buildSystemDevice(cqg_system& s) {
   sd.diagF = reinterpret_cast<const float2*>(b + oDiagF);
   sd.valF = reinterpret_cast<const float2*>(b + oValF);
   sd.jvalF = reinterpret_cast<const float2*>(b + oJvalF);
+  sd.Dp = warpTables ? int(Dp) : 0;
+  sd.wcol = warpTables ? reinterpret_cast<const int*>(b + oWcol) : nullptr;
+  sd.wdiagD = warpTables ? reinterpret_cast<const double2*>(b + oWdiagD) : nullptr;
+  sd.wvalD = warpTables ? reinterpret_cast<const double2*>(b + oWvalD) : nullptr;
+  sd.wdiagF = warpTables ? reinterpret_cast<const float2*>(b + oWdiagF) : nullptr;
+  sd.wvalF = warpTables ? reinterpret_cast<const float2*>(b + oWvalF) : nullptr;
+  sd.wjw = warpTables ? reinterpret_cast<const double*>(b + oWjw) : nullptr;
+  sd.wlambda = wlambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oWlambda);
+  sd.wfIdx = wfIdx.empty() ? nullptr : reinterpret_cast<const unsigned short*>(b + oWfIdx);
+  sd.wfreq = wfreq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oWfreq);
 }
 
 // ---- kernel dispatch -------------------------------------------------------------
@@ -1339,6 +1404,59 @@ int cqg_ensemble_get_jumps(const cqg_ensemble* ens, int64_t i, int32_t cap, doub
       if (lindblads) lindblads[w] = ll[k % J];
     }
     if (n_out) *n_out = w;
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_get_jump_rings(const cqg_ensemble* ens, int32_t* cap, uint64_t* counts, double* times,
+                                int32_t* lindblads) {
+  return guardedCuda([&] {
+    if (!ens) return fail(CQG_E_INVALID, "null ensemble");
+    ck(cudaSetDevice(ens->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(ens->stream), "cudaStreamSynchronize");
+    const size_t n = size_t(ens->nTraj), J = size_t(ens->jumpCap);
+    if (cap) *cap = ens->jumpCap;
+    if (counts) ck(cudaMemcpy(counts, ens->td.jumpN, n * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (times) ck(cudaMemcpy(times, ens->td.jumpT, n * J * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    if (lindblads) ck(cudaMemcpy(lindblads, ens->td.jumpL, n * J * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    return CQG_OK;
+  });
+}
+
+int cqg_ensemble_set_jump_capacity(cqg_ensemble* ens, int32_t cap) {
+  return guardedCuda([&] {
+    if (!ens || cap < 1) return fail(CQG_E_INVALID, "cqg_ensemble_set_jump_capacity: capacity >= 1 required");
+    if (cap == ens->jumpCap) return CQG_OK;
+    ck(cudaSetDevice(ens->device), "cudaSetDevice");
+    ck(cudaStreamSynchronize(ens->stream), "cudaStreamSynchronize");
+    const size_t n = size_t(ens->nTraj), J0 = size_t(ens->jumpCap), J1 = size_t(cap);
+    if (n * J1 > (size_t(1) << 31)) return fail(CQG_E_NOMEM, "cqg_ensemble_set_jump_capacity: capacity too large");
+    std::vector<unsigned long long> cnt(n);
+    std::vector<double> t0(n * J0), t1(n * J1, 0.);
+    std::vector<int> l0(n * J0), l1(n * J1, 0);
+    ck(cudaMemcpy(cnt.data(), ens->td.jumpN, n * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    ck(cudaMemcpy(t0.data(), ens->td.jumpT, n * J0 * 8, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    ck(cudaMemcpy(l0.data(), ens->td.jumpL, n * J0 * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+    // the most recent records that both rings hold, each at its slot (k mod capacity)
+    for (size_t i = 0; i < n; ++i) {
+      const unsigned long long keep = std::min<unsigned long long>(cnt[i], std::min(J0, J1));
+      for (unsigned long long k = cnt[i] - keep; k < cnt[i]; ++k) {
+        t1[i * J1 + k % J1] = t0[i * J0 + k % J0];
+        l1[i * J1 + k % J1] = l0[i * J0 + k % J0];
+      }
+    }
+    const size_t bytes = n * J1 * 12;
+    void* ring = cqg::engine::deviceAlloc(bytes, "cudaMalloc(jump rings)");
+    char* r = static_cast<char*>(ring);
+    ck(cudaMemcpy(r, t1.data(), n * J1 * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+    ck(cudaMemcpy(r + n * J1 * 8, l1.data(), n * J1 * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+    cqg::engine::deviceRelease(ens->device, ens->dJumpRing, ens->jumpRingBytes);
+    ens->dJumpRing = ring;
+    ens->jumpRingBytes = bytes;
+    ens->jumpCap = cap;
+    ens->td.jumpT = reinterpret_cast<double*>(r);
+    ens->td.jumpL = reinterpret_cast<int*>(r + n * J1 * 8);
+    ens->td.jumpCap = cap;
     return CQG_OK;
   });
 }

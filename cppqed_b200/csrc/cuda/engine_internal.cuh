@@ -106,9 +106,6 @@ inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors, int phase
 // Phase-table capacity a CTA-kernel group needs for one of its systems
 inline int blockPhaseElems(const dev::SysDev& sd) { return sd.hasFreq && sd.fIdx ? sd.nFD : 0; }
 
-// the off-diagonal slot bound of the warp kernel instance that serves smax slots
-inline int warpSlotInstance(int smax) { return smax <= 2 ? 2 : smax <= 4 ? 4 : 8; }
-
 // One persistent launch of group g over td on stream st (ra.order / nTasks / queue set by
 // the caller); allocates or grows the group's block-kernel scratch.
 void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGroup& g, dev::RunArgs ra, int nSM,

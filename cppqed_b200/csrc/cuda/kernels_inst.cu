@@ -18,13 +18,17 @@ namespace dev {
 
 using KernelFn = void (*)(TrajDev, RunArgs);
 
+// The instance reads exactly SMAX slots of the padded tables (a system with fewer slots
+// reads zero coefficients in the rest): 2 (a driven mode), 3 (Jaynes-Cummings), 4, 8.
 KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax, bool ip) {
   if (ip) {
     if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, true>;
+    if (smax <= 3) return &mcwfWarpKernel<CQG_REAL, CQG_E, 3, true>;
     if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, true>;
     return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, true>;
   }
   if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, false>;
+  if (smax <= 3) return &mcwfWarpKernel<CQG_REAL, CQG_E, 3, false>;
   if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, false>;
   return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, false>;
 }

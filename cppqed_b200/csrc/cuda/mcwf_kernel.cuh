@@ -33,6 +33,8 @@ constexpr unsigned short kNoPhase = 0xffff;
 // phases of each distinct frequency of the table, stage-major
 constexpr int kWarpPhaseElems = 5 * kWarpPhaseTableMax;
 constexpr unsigned FULL = 0xffffffffu;
+// off-diagonal slots of the warp kernel's padded tables
+constexpr int kWarpSlots = 8;
 
 // ---- complex helpers ---------------------------------------------------------
 template <typename R>
@@ -207,6 +209,20 @@ struct SysDev {
   const unsigned short* fIdx;  // [S][D] index of freq into fDist (kNoPhase: zero), or null
   const double2* fDist;  // [nFD]
   const double2* lambda; // [D] (Exact) or null
+  // Warp-kernel copies of the hot tables (D <= 128, S <= 8; null otherwise): rows padded to
+  // Dp = 32 ceil(D / 32), slots padded to kWarpSlots, padding with zero coefficients, its own
+  // row as column, no interaction-picture phase and zero rate weight and Exact exponent, so
+  // that a warp's rows and slots need no validity tests.
+  int Dp;
+  const int* wcol;             // [kWarpSlots][Dp]
+  const double2* wdiagD;       // [Dp]
+  const double2* wvalD;        // [kWarpSlots][Dp]
+  const float2* wdiagF;
+  const float2* wvalF;
+  const double* wjw;           // [nJ][Dp]
+  const double2* wlambda;      // [Dp] (Exact) or null
+  const unsigned short* wfIdx; // [kWarpSlots][Dp] (IP with a table) or null
+  const double2* wfreq;        // [kWarpSlots][Dp] (IP) or null
   // precision-specific copies
   const double2* diagD;
   const double2* valD;
@@ -223,12 +239,16 @@ struct Tables<double> {
   __device__ static const double2* diag(const SysDev& s) { return s.diagD; }
   __device__ static const double2* val(const SysDev& s) { return s.valD; }
   __device__ static const double2* jval(const SysDev& s) { return s.jvalD; }
+  __device__ static const double2* wdiag(const SysDev& s) { return s.wdiagD; }
+  __device__ static const double2* wval(const SysDev& s) { return s.wvalD; }
 };
 template <>
 struct Tables<float> {
   __device__ static const float2* diag(const SysDev& s) { return s.diagF; }
   __device__ static const float2* val(const SysDev& s) { return s.valF; }
   __device__ static const float2* jval(const SysDev& s) { return s.jvalF; }
+  __device__ static const float2* wdiag(const SysDev& s) { return s.wdiagF; }
+  __device__ static const float2* wval(const SysDev& s) { return s.wvalF; }
 };
 
 struct TrajDev {
@@ -308,6 +328,8 @@ struct Worker {
   const int lane;
   int D, S, nJ;
   bool hasH, hasEx, hasFreq, anySpecial;
+  // the padded warp tables (SysDev::wcol ...): row stride DMAX, no validity tests
+  static constexpr int DMAX = 32 * E;
   const int* col;
   const C2* val;
   const double2* freq;
@@ -350,12 +372,12 @@ struct Worker {
     hasH = s->hasH != 0;
     hasEx = s->hasEx != 0;
     hasFreq = s->hasFreq != 0;
-    col = s->col;
-    val = Tables<R>::val(*s);
-    freq = s->freq;
-    phsTab = ph && s->fIdx && s->nFD <= kWarpPhaseTableMax;
-    fIdx = s->fIdx;
-    jw = s->jw;
+    col = s->wcol;
+    val = Tables<R>::wval(*s);
+    freq = s->wfreq;
+    phsTab = ph && s->wfIdx && s->nFD <= kWarpPhaseTableMax;
+    fIdx = s->wfIdx;
+    jw = s->wjw;
     anySpecial = false;
     for (int m = 0; m < nJ; ++m) anySpecial |= !s->jHasW[m];
   }
@@ -364,18 +386,16 @@ struct Worker {
   __device__ __forceinline__ bool valid(int e) const { return row(e) < D; }
 
   __device__ __forceinline__ void loadOperator() {
-    const C2* dg = Tables<R>::diag(*sysp);
+    const C2* dg = Tables<R>::wdiag(*sysp);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int r = row(e);
-      const bool v = r < D;
-      diag[e] = v ? dg[r] : mk<C2>(0, 0);
+      diag[e] = dg[r];
       if constexpr (CREG) {
 #pragma unroll
         for (int s = 0; s < SMAX; ++s) {
-          const bool vs = v && s < S;
-          ccol[s][e] = vs ? col[s * D + r] : 0;
-          cval[s][e] = vs ? val[s * D + r] : mk<C2>(0, 0);
+          ccol[s][e] = col[s * DMAX + r];
+          cval[s][e] = val[s * DMAX + r];
         }
       } else {
 #pragma unroll
@@ -384,7 +404,7 @@ struct Worker {
 #pragma unroll
           for (int b = 0; b < 4; ++b) {
             const int s = 4 * w + b;
-            if (s < SMAX && v && s < S) p |= unsigned(col[s * D + r]) << (8 * b);
+            if (s < SMAX) p |= unsigned(col[s * DMAX + r]) << (8 * b);
           }
           cpack[w][e] = p;
         }
@@ -411,45 +431,45 @@ struct Worker {
   // out = (H/i) y at picture time tau; y staged through `buf`
 
   // out = (H/i) y at picture time tau = stage time - t0 (stage 0..5 of the attempt)
+  // Every row and slot of the padded tables is read: padding rows hold zeros and padding
+  // slots a zero coefficient on the row itself, so there is no branch in the slot loops and
+  // the loads of a right-hand side can all be issued ahead of their FMAs.
   __device__ __forceinline__ void rhs(const C2 (&y)[E], C2 (&out)[E], double tau, int stage, C2* buf) {
 #pragma unroll
-    for (int e = 0; e < E; ++e)
-      if (valid(e)) buf[row(e)] = y[e];
+    for (int e = 0; e < E; ++e) buf[row(e)] = y[e];
     __syncwarp();
     ++nRhs;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       C2 acc = cmul(diag[e], y[e]);
-      const int r = valid(e) ? row(e) : 0;
+      const int r = row(e);
 #pragma unroll
       for (int s = 0; s < SMAX; ++s) {
-        if (s < S) {
-          C2 c;
-          int cc;
-          if constexpr (CREG) {
-            c = cval[s][e];
-            cc = ccol[s][e];
+        C2 c;
+        int cc;
+        if constexpr (CREG) {
+          c = cval[s][e];
+          cc = ccol[s][e];
+        } else {
+          c = __ldg(&val[s * DMAX + r]);
+          cc = int((cpack[s >> 2][e] >> (8 * (s & 3))) & 0xffu);
+        }
+        if (IP && hasFreq) {
+          if (phsOn) {
+            if (stage) {
+              const unsigned k = __ldg(&fIdx[s * DMAX + r]);
+              const double2 ph = k == kNoPhase ? make_double2(1., 0.) : phs[(stage - 1) * kWarpPhaseTableMax + k];
+              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+            }
           } else {
-            c = valid(e) ? __ldg(&val[s * D + r]) : mk<C2>(0, 0);
-            cc = int((cpack[s >> 2][e] >> (8 * (s & 3))) & 0xffu);
-          }
-          if (IP && hasFreq && valid(e)) {
-            if (phsOn) {
-              if (stage) {
-                const unsigned k = __ldg(&fIdx[s * D + r]);
-                const double2 ph = k == kNoPhase ? make_double2(1., 0.) : phs[(stage - 1) * kWarpPhaseTableMax + k];
-                c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
-              }
-            } else {
-              const double2 f = __ldg(&freq[s * D + r]);
-              if ((f.x != 0. || f.y != 0.) && tau != 0.) {  // exp(0 f) = 1 exactly
-                const double2 ph = cexpScaled(tau, f);
-                c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
-              }
+            const double2 f = __ldg(&freq[s * DMAX + r]);
+            if ((f.x != 0. || f.y != 0.) && tau != 0.) {  // exp(0 f) = 1 exactly
+              const double2 ph = cexpScaled(tau, f);
+              c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
             }
           }
-          acc = cfma(c, buf[cc], acc);
         }
+        acc = cfma(c, buf[cc], acc);
       }
       out[e] = acc;
     }
@@ -519,8 +539,8 @@ struct Worker {
         y[e] = axpy(b5, k5[e], axpy(b3, k3[e], axpy(b2, k2[e], axpy(b0, k0[e], x[e]))));
         C2 xe = mk<C2>(0, 0);
         xe = axpy(e5, k5[e], axpy(e4, k4[e], axpy(e3, k3[e], axpy(e2, k2[e], axpy(e0, k0[e], xe)))));
-        if (valid(e))
-          errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(x[e]) + adt * cabs(k0[e])));
+        // a padding row (all zero) never raises the maximum
+        errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(x[e]) + adt * cabs(k0[e])));
       }
       double err = warpMax(errLocal.value());
       if (!(err == err)) {  // NaN error norm
@@ -576,11 +596,10 @@ struct Worker {
     if (hasEx) {
       const double tau = t - t0;
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        if (valid(e)) {
-          const double2 u = cexpScaled(tau, __ldg(&sysp->lambda[row(e)]));
-          x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
-        }
+      for (int e = 0; e < E; ++e) {
+        const double2 u = cexpScaled(tau, __ldg(&sysp->wlambda[row(e)]));
+        x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
+      }
       t0 = t;
     }
     double red[MAX_JUMPS + 1];
@@ -591,8 +610,7 @@ struct Worker {
     if (li) {
       if (anySpecial) {
 #pragma unroll
-        for (int e = 0; e < E; ++e)
-          if (valid(e)) buf0[row(e)] = x[e];
+        for (int e = 0; e < E; ++e) buf0[row(e)] = x[e];
         __syncwarp();
       }
 #pragma unroll
@@ -600,10 +618,9 @@ struct Worker {
         red[m + 1] = 0.;
         if (m < nJ) {
           if (!anySpecial || sysp->jHasW[m]) {
-            const double* w = jw + size_t(m) * D;
+            const double* w = jw + size_t(m) * DMAX;
 #pragma unroll
-            for (int e = 0; e < E; ++e)
-              if (valid(e)) red[m + 1] += __ldg(&w[row(e)]) * abs2(x[e]);
+            for (int e = 0; e < E; ++e) red[m + 1] += __ldg(&w[row(e)]) * abs2(x[e]);
           } else {
             C2 jx[E];
             applyJump(m, buf0, jx);
@@ -699,8 +716,7 @@ struct Worker {
       }
     if (random < 0) {
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        if (valid(e)) buf0[row(e)] = x[e];
+      for (int e = 0; e < E; ++e) buf0[row(e)] = x[e];
       __syncwarp();
       C2 jx[E];
       applyJump(lindbladNo, buf0, jx);
@@ -730,8 +746,7 @@ struct Worker {
     const double tCache = t, dtDidCache = dtDid;
     if (li) {
 #pragma unroll
-      for (int e = 0; e < E; ++e)
-        if (valid(e)) cache[row(e)] = x[e];
+      for (int e = 0; e < E; ++e) cache[row(e)] = x[e];
     }
     double rates[MAX_JUMPS];
     if (!coherentAndRates(Dt, li, rates)) return false;
@@ -743,8 +758,7 @@ struct Worker {
           return false;
         }
 #pragma unroll
-        for (int e = 0; e < E; ++e)
-          if (valid(e)) x[e] = cache[row(e)];
+        for (int e = 0; e < E; ++e) x[e] = cache[row(e)];
         if (!coherentAndRates(Dt, li, rates)) return false;
       }
       if (!performJump(rates, td)) return false;
@@ -756,8 +770,7 @@ struct Worker {
   // per-trajectory linear averages <psi|O_k|psi> (output times only)
   __device__ __forceinline__ void averages(double* out) {
 #pragma unroll
-    for (int e = 0; e < E; ++e)
-      if (valid(e)) buf0[row(e)] = x[e];
+    for (int e = 0; e < E; ++e) buf0[row(e)] = x[e];
     __syncwarp();
     const int nObs = sysp->nObs, SO = sysp->SO;
     for (int k = 0; k < nObs; ++k) {

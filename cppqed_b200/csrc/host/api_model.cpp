@@ -90,6 +90,32 @@ int cqg_model_key(const cqg_model* m, char* buf, size_t cap) {
   return CQG_OK;
 }
 
+namespace {
+int copyText(const std::string& s, char* buf, size_t cap, size_t* needed) {
+  if (needed) *needed = s.size() + 1;
+  if (!buf) return CQG_OK;
+  if (!cap) return cqg::fail(CQG_E_INVALID, "zero capacity");
+  std::strncpy(buf, s.c_str(), cap - 1);
+  buf[cap - 1] = 0;
+  return CQG_OK;
+}
+}  // namespace
+
+int cqg_model_key_text(const cqg_model* m, int32_t first_column, char* buf, size_t cap, size_t* needed) {
+  if (!m) return cqg::fail(CQG_E_INVALID, "null argument");
+  return guarded([&] { return copyText(m->m->sys->keyText(first_column), buf, cap, needed); });
+}
+
+int cqg_model_parameters_text(const cqg_model* m, char* buf, size_t cap, size_t* needed) {
+  if (!m) return cqg::fail(CQG_E_INVALID, "null argument");
+  return guarded([&] { return copyText(m->m->sys->parametersText(), buf, cap, needed); });
+}
+
+int cqg_model_command_line(const cqg_model* m, char* buf, size_t cap, size_t* needed) {
+  if (!m) return cqg::fail(CQG_E_INVALID, "null argument");
+  return guarded([&] { return copyText(m->m->commandLine, buf, cap, needed); });
+}
+
 int cqg_model_destroy(cqg_model* m) {
   delete m;
   return CQG_OK;

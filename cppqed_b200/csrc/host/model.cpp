@@ -2,6 +2,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <sstream>
 
 namespace cqg {
 
@@ -39,6 +41,7 @@ System System::free(const ElementPtr& f) {
 System System::binary(const ElementPtr& ia) {
   if (ia->frees.size() != 2) throw std::invalid_argument("binary::make needs a binary interaction");
   System s;
+  s.binary_ = true;
   s.dims_ = {ia->frees[0]->dims.at(0), ia->frees[1]->dims.at(0)};
   s.placed_.push_back({ia->frees[0], {0}, 0});
   s.placed_.push_back({ia->frees[1], {1}, 0});
@@ -207,6 +210,50 @@ EvolutionPars::EvolutionPars(ParameterTable& p) {
   if (evol == "master" && picture == Picture::IP) picture = Picture::UIP;  // QM_Picture.cc:41-50
   prec = p.add<std::string>("enginePrecision", m, "fp64");
   rng = p.add<std::string>("rng", m, "pcg64");
+}
+
+std::string System::keyText(int firstColumn) const {
+  std::ostringstream os;
+  if (binary_) os << "Binary system\n";  // binary::streamKey (BinarySystem.cc:120-127)
+  int col = firstColumn;
+  for (auto& p : placed_) {
+    if (p.e->avLabels.empty()) continue;
+    os << p.e->keyTitle << "\n";
+    for (auto& l : p.e->avLabels) {
+      char num[16];
+      std::snprintf(num, sizeof num, "%2d. ", col++);
+      os << num << l << "\n";
+    }
+  }
+  return os.str();
+}
+
+std::string System::parametersText() const {
+  std::ostringstream os;
+  for (auto& p : placed_) {
+    std::string t = p.e->parsStream;
+    if (t.empty()) t = p.e->keyTitle + "\n";
+    if (t.back() != '\n') t += "\n";
+    os << t;
+    if (p.axes.size() == 1) os << "Dimension: " << dims_[p.axes[0]] << "\n";
+    os << "\n";
+  }
+  os << "System characteristics: " << (isExact() ? "Interaction picture, " : "")
+     << (isHamiltonian() ? "Hamiltonian evolution, " : "") << (isLiouvillean() ? "Liouvillean evolution, " : "")
+     << (nAvr_ ? "calculates Averages." : "no Averages.") << "\n";
+  os << "Decay channels:\n";
+  int ordinal = 0;
+  for (auto& p : placed_) {
+    if (p.e->jumps.empty()) continue;
+    os << p.e->keyTitle << "\n";
+    for (auto& j : p.e->jumps) {
+      char num[16];
+      std::snprintf(num, sizeof num, "%2d. ", ordinal++);
+      os << num << (j.label.empty() ? std::string("jump") : j.label) << "\n";
+    }
+  }
+  os << "Alternative Lindblads: none\n";
+  return os.str();
 }
 
 }  // namespace cqg

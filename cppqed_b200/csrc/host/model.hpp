@@ -40,6 +40,15 @@ class System {
   // Applies every element's process_v on its own column range (BinarySystem.cc:73-98).
   void process(double* averages) const;
 
+  // The system's part of the "Key to data" block (LiouvilleanAveragedCommon.h:82-93,
+  // KeyPrinter): per averaging element its title, then its columns numbered from
+  // firstColumn (" 3. rho00"), one line each.
+  std::string keyText(int firstColumn) const;
+  // The system's parameter block of a trajectory file's header (Structure.h:178-186,
+  // streamParameters): every element's description, the dimension, the system's
+  // characteristics and the decay channels in ordinal order, one line each.
+  std::string parametersText() const;
+
   // The descriptor view; pointers stay valid for the lifetime of this object.
   const cqg_system_desc& desc() const { return desc_; }
 
@@ -57,6 +66,7 @@ class System {
     int colOffset;
   };
   std::vector<Placed> placed_;  // frees (one per axis) then acts
+  bool binary_ = false;         // binary::make: its key opens with "Binary system"
   std::vector<size_t> dims_;
   int nAvr_ = 0;
   double highestFrequency_ = 0;

@@ -245,6 +245,23 @@ class Ensemble:
                                            l.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(n)))
         return t[:n.value], l[:n.value]
 
+    def set_jump_capacity(self, cap):
+        """Per-trajectory capacity of the jump record rings (default 64)."""
+        check(lib().cqg_ensemble_set_jump_capacity(self._h, int(cap)))
+
+    def jump_rings(self):
+        """(counts [n_traj], times [n_traj, cap], lindblads [n_traj, cap]): every ring at once;
+        the k-th jump of trajectory i is at slot k % cap while k >= counts[i] - cap."""
+        cap = C.c_int32()
+        check(lib().cqg_ensemble_get_jump_rings(self._h, C.byref(cap), None, None, None))
+        counts = np.zeros(self.n_traj, dtype=np.uint64)
+        times = np.zeros((self.n_traj, cap.value))
+        lind = np.zeros((self.n_traj, cap.value), dtype=np.int32)
+        check(lib().cqg_ensemble_get_jump_rings(self._h, None, counts.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                times.ctypes.data_as(C.POINTER(C.c_double)),
+                                                lind.ctypes.data_as(C.POINTER(C.c_int32))))
+        return counts, times, lind
+
     def status(self):
         b = C.c_uint32()
         rc = lib().cqg_ensemble_status(self._h, C.byref(b))

@@ -247,6 +247,16 @@ int cqg_ensemble_get_logger_maxima(const cqg_ensemble* ens, double* max_overshoo
 int cqg_ensemble_get_jumps(const cqg_ensemble* ens, int64_t i, int32_t cap, double* times,
                            int32_t* lindblads, int32_t* n_out);
 
+/* Every trajectory's jump ring at once, for a host that keeps all jump records (the ensemble
+ * log's histogram of jump times, MCWF_TrajectoryLogger.cc:79-121): *cap (per-trajectory ring
+ * capacity), counts[i] (jumps of trajectory i so far; its k-th jump is at slot k mod cap
+ * while k >= counts[i] - cap), times and lindblads [n_traj][cap].  Any pointer may be NULL. */
+int cqg_ensemble_get_jump_rings(const cqg_ensemble* ens, int32_t* cap, uint64_t* counts, double* times,
+                                int32_t* lindblads);
+/* Changes the per-trajectory ring capacity (default 64), keeping the most recent records.
+ * A checkpoint loads only into an ensemble with the capacity it was saved with. */
+int cqg_ensemble_set_jump_capacity(cqg_ensemble* ens, int32_t cap);
+
 /* OR of all trajectory status bits; CQG_E_NONFINITE / CQG_E_STALLED when set. */
 int cqg_ensemble_status(const cqg_ensemble* ens, uint32_t* bits);
 

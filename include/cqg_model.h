@@ -49,6 +49,15 @@ int cqg_model_n_avr(const cqg_model* m, int32_t* n_avr);
 int cqg_model_process(const cqg_model* m, double* averages);
 /* Column labels ("Key to data"), '\n'-separated, NUL-terminated. */
 int cqg_model_key(const cqg_model* m, char* buf, size_t cap);
+/* Text for a reference-format trajectory file header (trajectory::run's introduction,
+ * Trajectory.h:535-545): the system's part of "Key to data" with its columns numbered from
+ * first_column (each averaging element's title, then " 3. rho00" lines), the system's
+ * parameter block (element descriptions, dimensions, characteristics, decay channels), and
+ * the command line the model was built from.  Lines end in '\n'.  buf == NULL only reports
+ * the size needed (with the NUL) in *needed; otherwise at most cap - 1 characters are copied. */
+int cqg_model_key_text(const cqg_model* m, int32_t first_column, char* buf, size_t cap, size_t* needed);
+int cqg_model_parameters_text(const cqg_model* m, char* buf, size_t cap, size_t* needed);
+int cqg_model_command_line(const cqg_model* m, char* buf, size_t cap, size_t* needed);
 int cqg_model_destroy(cqg_model* m);
 
 #ifdef __cplusplus

@@ -2,7 +2,8 @@
 
 Reads Testing/expected/run_<name> (C++QED v2.120, written by CPPQEDscripts with the
 command lines of Testing/run/testdriver.conf) and stores, per run, the command line,
-the streamed rows (time, dtDid, averages), the numbers of the end-of-run ensemble log
+the streamed rows (time, dtDid, averages), the system's lines of the header's key to the
+columns, the numbers of the end-of-run ensemble log
 (mcwf::EnsembleLogger::stream: average steps, dpLimit / dpTolerance overshoots with their
 maxima, maximal norm deviation, average jumps) and the pcg64 engine state serialised in
 the first archive of the matching .state file (the engine right after seeding).
@@ -31,6 +32,21 @@ LOG_PATTERNS = {
     "max_norm_deviation": r"Maximal deviation of norm from 1: (\S+)",
     "average_jumps": r"Average number of total jumps: (\S+)",
 }
+
+
+def parse_key(path):
+    """The system's part of the header's "Key to data" block: the lines after the
+    trajectory's own columns (time, dtDid) up to the next empty line, without the "# "."""
+    lines = [l.rstrip("\n") for l in open(path)]
+    try:
+        i = lines.index("#  2. dtDid") + 1
+    except ValueError:
+        return None
+    key = []
+    while i < len(lines) and lines[i].startswith("#"):
+        key.append(lines[i][2:])
+        i += 1
+    return key
 
 
 def parse(path):
@@ -73,7 +89,7 @@ def main(ref):
             i = args.index("--o")
             del args[i:i + 2]
         out[r] = {"script": os.path.basename(cmd.split()[0]), "args": args, "rows": rows,
-                  "pcg64_first_archive": pcg_state(p + ".state")}
+                  "pcg64_first_archive": pcg_state(p + ".state"), "key": parse_key(p)}
         if log:
             out[r]["ensemble_log"] = log
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_runs.json")

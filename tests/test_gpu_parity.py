@@ -764,3 +764,35 @@ def test_particle_position_averages_by_fast_transform_match_dense(gpu):
     dense = d_sums.cpu().numpy()
     assert np.allclose(fast, dense, rtol=1e-11, atol=1e-12), (fast, dense)
     assert abs(dense[6]) > 1e-3 and dense[7] > 1e-3  # <X> and <X^2> columns are not trivially zero
+
+
+def test_jump_capacity_change_keeps_the_most_recent_records(gpu):
+    """cqg_ensemble_set_jump_capacity: shrinking keeps the most recent records of every
+    trajectory at their slots; growing keeps all of them; records made afterwards are kept
+    as in an ensemble that had the capacity from the start (same streams)."""
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    sysd = gpu.System(model.desc)
+    pars = model.run_pars().mcwf
+    n = 32
+    ref = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ref.set_jump_capacity(4096)
+    ref.run(1.0, 2)
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    ens.run(1.0, 1)
+    ens.set_jump_capacity(4)
+    counts, times, _ = ens.jump_rings()
+    for i in range(n):
+        kept = min(int(counts[i]), 4)
+        want = ref.jumps(i, 4096)[0][:int(counts[i])][int(counts[i]) - kept:]
+        got = [times[i, k % 4] for k in range(int(counts[i]) - kept, int(counts[i]))]
+        assert np.array_equal(got, want)
+    ens.set_jump_capacity(4096)
+    ens.run(1.0, 1)
+    total = 0
+    for i in range(n):
+        c0 = int(counts[i])
+        t_ref = ref.jumps(i, 4096)[0]
+        t_got = ens.jumps(i, 4096)[0]
+        assert np.array_equal(t_got, t_ref[max(0, c0 - 4):]), i
+        total += len(t_ref) - c0
+    assert total > 0
