@@ -5,6 +5,7 @@ with g++, the CUDA sources with nvcc (``-gencode arch=compute_100a,code=sm_100a`
 and everything is linked into one shared library exporting the C ABI of
 ``include/cqg.h`` and ``include/cqg_model.h``.  Rebuilds only what is out of date.
 """
+import hashlib
 import os
 import subprocess
 import sys
@@ -42,6 +43,33 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _digest(files, cmd):
+    """Content hash of an object's inputs and its command line."""
+    h = hashlib.sha256(" ".join(cmd).encode())
+    for f in files:
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def _needs_compile(obj, files, cmd):
+    """An object is rebuilt unless its stamp holds the hash of the inputs it was compiled
+    from.  The hash is taken before the compiler starts, so a source edited while it compiles
+    leaves a stamp that no longer matches."""
+    d = _digest(files, cmd)
+    try:
+        with open(obj + ".stamp") as fh:
+            ok = os.path.exists(obj) and fh.read() == d
+    except OSError:
+        ok = False
+    return (not ok), d
+
+
+def _stamp(obj, d):
+    with open(obj + ".stamp", "w") as fh:
+        fh.write(d)
+
+
 def _run(cmd, verbose):
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -65,8 +93,11 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     for src in HOST_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
-        if _stale(o, [s] + deps(HOST_HEADERS)):
-            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", *inc, "-c", s, "-o", o], verbose)
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-Wall", *inc, "-c", s, "-o", o]
+        need, d = _needs_compile(o, [s] + deps(HOST_HEADERS), cmd)
+        if need:
+            _run(cmd, verbose)
+            _stamp(o, d)
         objs.append(o)
     info = ""
     jobs = []
@@ -81,19 +112,22 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     procs = []
     for s, o, defs, hdrs in jobs:
         objs.append(o)
-        if _stale(o, [s] + hdrs) or ptxas_info:
-            cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs,
-                   *extra_flags, "-c", s, "-o", o]
+        cmd = [_nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *inc, *defs,
+               *extra_flags, "-c", s, "-o", o]
+        need, d = _needs_compile(o, [s] + hdrs, cmd)
+        if need or ptxas_info:
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             if verbose:
                 print(" ".join(cmd), flush=True)
-            procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
-    for cmd, p in procs:
+            procs.append((cmd, o, d, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                                     text=True)))
+    for cmd, o, d, p in procs:
         out, _ = p.communicate()
         if p.returncode != 0:
             sys.stderr.write(out)
             raise RuntimeError("build step failed: " + " ".join(cmd[:3]) + " ...")
+        _stamp(o, d)
         info += out
     out = lib or LIB
     if _stale(out, objs):
