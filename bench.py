@@ -387,7 +387,7 @@ def run_ours(args, rank, world, dev):
                          MCWF_TRAFFIC["workload"], MCWF_TRAFFIC["precision"]) else None,
                      "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU",
                      "flops_per_attempt": per_attempt, "nnz_h": nnz},
-        "n_traj": n_traj, "model": model, "apply": apply,
+        "n_traj": n_traj, "model": model, "apply": apply, "plan": ens.plan(),
     }
 
 
@@ -837,7 +837,7 @@ def main():
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
-               "config": workload_config(args, world),
+               "config": dict(workload_config(args, world), kernel_groups=r["plan"]),
                "e2e": r["e2e"], "roofline": r["roofline"], "apply_roofline": r["apply"], "cpu_baseline": cpu,
                "clocks": r["clocks"],
                "gpu_launches": 3 * args.steps,

@@ -86,8 +86,8 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     inc = ["-I" + os.path.join(ROOT, "include")]
     public = [os.path.join(ROOT, "include", h) for h in ("cqg.h", "cqg_model.h")]
 
-    def deps(names):
-        return [os.path.join(CSRC, h) for h in names] + public
+    def deps(names, with_public=True):
+        return [os.path.join(CSRC, h) for h in names] + (public if with_public else [])
 
     objs = []
     for src in HOST_SOURCES:
@@ -108,7 +108,7 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
     inst = os.path.join(CSRC, "cuda", "kernels_inst.cu")
     for r, e in KERNEL_INSTANCES:
         jobs.append((inst, os.path.join(OBJDIR, "kernels_%s_e%d.o" % (r, e)),
-                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e], deps(KERNEL_HEADERS)))
+                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e], deps(KERNEL_HEADERS, with_public=False)))
     procs = []
     for s, o, defs, hdrs in jobs:
         objs.append(o)

@@ -56,6 +56,9 @@ class HostStaging {
 };
 
 // single device allocation carved into aligned sub-buffers
+// autotuner shape bit: the warp kernel's instance compiled for more resident CTAs
+constexpr int kHighOccupancyFlag = 1 << 17;
+
 struct Arena {
   std::vector<std::pair<size_t, size_t>> parts;  // offset, size
   size_t total = 0;
@@ -474,14 +477,14 @@ using KernelFn = void (*)(dev::TrajDev, dev::RunArgs);
 
 namespace cqg {
 namespace dev {
-KernelFn pick_double_e1(int smax, bool ip);
-KernelFn pick_double_e2(int smax, bool ip);
-KernelFn pick_double_e3(int smax, bool ip);
-KernelFn pick_double_e4(int smax, bool ip);
-KernelFn pick_float_e1(int smax, bool ip);
-KernelFn pick_float_e3(int smax, bool ip);
-KernelFn pick_float_e2(int smax, bool ip);
-KernelFn pick_float_e4(int smax, bool ip);
+KernelFn pick_double_e1(int smax, bool ip, bool highOccupancy);
+KernelFn pick_double_e2(int smax, bool ip, bool highOccupancy);
+KernelFn pick_double_e3(int smax, bool ip, bool highOccupancy);
+KernelFn pick_double_e4(int smax, bool ip, bool highOccupancy);
+KernelFn pick_float_e1(int smax, bool ip, bool highOccupancy);
+KernelFn pick_float_e3(int smax, bool ip, bool highOccupancy);
+KernelFn pick_float_e2(int smax, bool ip, bool highOccupancy);
+KernelFn pick_float_e4(int smax, bool ip, bool highOccupancy);
 }  // namespace dev
 }  // namespace cqg
 
@@ -503,16 +506,16 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
                  const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars);
 bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device);
 
-KernelFn pickKernel(bool fp64, int E, int SMAX, bool ip) {
+KernelFn pickKernel(bool fp64, int E, int SMAX, bool ip, bool hi) {
   if (fp64)
-    return E == 1 ? dev::pick_double_e1(SMAX, ip)
-         : E == 2 ? dev::pick_double_e2(SMAX, ip)
-         : E == 3 ? dev::pick_double_e3(SMAX, ip)
-                  : dev::pick_double_e4(SMAX, ip);
-  return E == 1 ? dev::pick_float_e1(SMAX, ip)
-       : E == 2 ? dev::pick_float_e2(SMAX, ip)
-       : E == 3 ? dev::pick_float_e3(SMAX, ip)
-                : dev::pick_float_e4(SMAX, ip);
+    return E == 1 ? dev::pick_double_e1(SMAX, ip, hi)
+         : E == 2 ? dev::pick_double_e2(SMAX, ip, hi)
+         : E == 3 ? dev::pick_double_e3(SMAX, ip, hi)
+                  : dev::pick_double_e4(SMAX, ip, hi);
+  return E == 1 ? dev::pick_float_e1(SMAX, ip, hi)
+       : E == 2 ? dev::pick_float_e2(SMAX, ip, hi)
+       : E == 3 ? dev::pick_float_e3(SMAX, ip, hi)
+                : dev::pick_float_e4(SMAX, ip, hi);
 }
 
 __global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, int nAvrStride, int nAvr,
@@ -780,6 +783,9 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     if (g.threads % 32 || g.threads < 32 || g.threads > (g.kind ? 512 : 128))
       return fail(CQG_E_INVALID, "ensemble: cta_threads must be a multiple of 32, at most 128 (warp kernel) or 512");
     g.smemVectors = pars->cta_threads > 0 && pars->cta_shared_vectors && sharedVectorsFit(g, e->elemBytes, e->device);
+    g.highOccupancy = g.kind == 0 && pars->cta_threads > 0 && pars->cta_shared_vectors &&
+                      dev::warpHighOccupancyVariant(g.E, g.smax <= 2 ? 2 : g.smax <= 3 ? 3 : g.smax <= 4 ? 4 : 8,
+                                                    g.anyFreq);
     g.phaseTable = pars->ip_phase_table >= 0;
     if (!g.phaseTable || g.kind == 0) g.phaseElems = 0;
   }
@@ -787,7 +793,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
     for (size_t gi = 0; gi < e->groups.size(); ++gi) {
       const int shape = tunedThreads(*e, gi, systems, nSys, psi0s, psi0Off, *pars);
       e->groups[gi].threads = shape & 0xffff;
-      e->groups[gi].smemVectors = (shape >> 16) != 0;
+      e->groups[gi].smemVectors = (shape & (1 << 16)) != 0;
+      e->groups[gi].highOccupancy = (shape & kHighOccupancyFlag) != 0;
     }
   *out = e.release();
   return CQG_OK;
@@ -802,11 +809,12 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
                  cudaStream_t st) {
   dev::TrajDev tdArg = td;
   if (g.kind == 0) {
-    KernelFn fn = pickKernel(fp64, g.E, g.smax, g.anyFreq);
+    KernelFn fn = pickKernel(fp64, g.E, g.smax, g.anyFreq, g.highOccupancy);
     const int warps = g.threads / 32;
     // stage vectors, warp scratch, and for interaction-picture systems the phase tables
     ra.phaseCache = g.anyFreq && g.phaseTable ? 1 : 0;
-    const size_t smem = size_t(warps) * 3 * 32 * g.E * elemBytes + size_t(warps) * sizeof(dev::WarpScratch) +
+    const size_t smem = size_t(warps) * dev::warpSmemVectors(g.E) * 32 * g.E * elemBytes +
+                        size_t(warps) * sizeof(dev::WarpScratch) +
                         (ra.phaseCache ? size_t(warps) * dev::kWarpPhaseElems * sizeof(double2) : 0);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
@@ -954,10 +962,16 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
 // same initial states, so the ensemble itself is not advanced) over a fixed number of MCWF
 // steps each, and the fastest is kept.  Results are cached per (device, precision, kernel kind, rows per lane, slot
 // bound, largest dimension) for the life of the process.
-// Candidate shapes, encoded as CTA threads | (shared-memory stage vectors << 16).
+// Candidate shapes, encoded as CTA threads | (shared-memory stage vectors << 16) | (the warp
+// kernel's high-occupancy instance << 17).
 std::vector<int> threadCandidates(const KernelGroup& g, bool vectorsFit) {
   std::vector<int> c;
-  if (g.kind == 0) return {64, 128};
+  if (g.kind == 0) {  // warp kernel: CTA size, and the high-occupancy instance where there is one
+    c = {64, 128};
+    if (dev::warpHighOccupancyVariant(g.E, g.smax <= 2 ? 2 : g.smax <= 3 ? 3 : g.smax <= 4 ? 4 : 8, g.anyFreq))
+      c.insert(c.end(), {64 | kHighOccupancyFlag, 128 | kHighOccupancyFlag});
+    return c;
+  }
   for (int q = 1; q <= 4; ++q) {  // rows per thread
     const int t = std::min(512, std::max(64, ((g.Dmax + q - 1) / q + 31) / 32 * 32));
     if (std::find(c.begin(), c.end(), t) == c.end()) c.push_back(t);
@@ -1021,7 +1035,8 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   for (int pass = 0; pass < 2; ++pass)  // pass 0 warms up every candidate
     for (int c : cands) {
       tmp->groups[0].threads = c & 0xffff;
-      tmp->groups[0].smemVectors = (c >> 16) != 0;
+      tmp->groups[0].smemVectors = (c & (1 << 16)) != 0;
+      tmp->groups[0].highOccupancy = (c & kHighOccupancyFlag) != 0;
       ra.nSteps = pass ? 12 : 2;
       if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
       if (pass && (bestMs == 0 || tmp->lastMs < bestMs)) {
@@ -1291,7 +1306,7 @@ int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan,
   for (int32_t g = 0; g < std::min<int32_t>(cap, *n_groups); ++g) {
     const KernelGroup& k = ens->groups[g];
     int32_t* o = plan + 5 * g;
-    o[0] = k.kind == 1 && k.smemVectors ? 2 : k.kind;
+    o[0] = k.kind == 1 && k.smemVectors ? 2 : k.kind == 0 && k.highOccupancy ? 3 : k.kind;
     o[1] = k.E;
     o[2] = k.smax;
     o[3] = k.threads;

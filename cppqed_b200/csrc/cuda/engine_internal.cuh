@@ -81,6 +81,7 @@ struct KernelGroup {
   int Dmax = 0;
   bool anyFreq = false;  // some system of the group has interaction-picture frequencies
   bool smemVectors = false;  // CTA kind: stage derivatives in shared memory instead of scratch
+  bool highOccupancy = false;  // warp kind: the instance compiled for more resident CTAs
   bool phaseTable = true;    // interaction picture: phases from the systems' tables of
                              // distinct frequencies where they have one
   int phaseElems = 0;        // CTA kind: shared-memory phase table capacity (max over systems)

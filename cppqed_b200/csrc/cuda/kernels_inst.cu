@@ -1,6 +1,7 @@
 // Explicit instantiation of the fused MCWF warp kernel for one (precision, rows per
 // lane) pair; the build compiles this file once per pair (-DCQG_REAL, -DCQG_E) so the
-// instances compile in parallel.  Exposes pick_<real>_e<E>(SMAX, interaction picture).
+// instances compile in parallel.  Exposes pick_<real>_e<E>(SMAX, interaction picture, high
+// occupancy).
 #include "mcwf_kernel.cuh"
 
 #ifndef CQG_REAL
@@ -20,17 +21,25 @@ using KernelFn = void (*)(TrajDev, RunArgs);
 
 // The instance reads exactly SMAX slots of the padded tables (a system with fewer slots
 // reads zero coefficients in the rest): 2 (a driven mode), 3 (Jaynes-Cummings), 4, 8.
-KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax, bool ip) {
-  if (ip) {
-    if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, true>;
-    if (smax <= 3) return &mcwfWarpKernel<CQG_REAL, CQG_E, 3, true>;
-    if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, true>;
-    return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, true>;
+// highOccupancy selects the instance compiled for more resident CTAs where there is one.
+template <int SMAX, bool IP>
+KernelFn pickOccupancy(bool highOccupancy) {
+  if constexpr (warpHighOccupancyVariant(CQG_E, SMAX, IP)) {
+    if (highOccupancy) return &mcwfWarpKernel<CQG_REAL, CQG_E, SMAX, IP, WarpMinBlocksHigh<CQG_E>::value>;
   }
-  if (smax <= 2) return &mcwfWarpKernel<CQG_REAL, CQG_E, 2, false>;
-  if (smax <= 3) return &mcwfWarpKernel<CQG_REAL, CQG_E, 3, false>;
-  if (smax <= 4) return &mcwfWarpKernel<CQG_REAL, CQG_E, 4, false>;
-  return &mcwfWarpKernel<CQG_REAL, CQG_E, 8, false>;
+  return &mcwfWarpKernel<CQG_REAL, CQG_E, SMAX, IP, WarpMinBlocks<CQG_E, IP>::value>;
+}
+
+template <bool IP>
+KernelFn pickSlots(int smax, bool highOccupancy) {
+  if (smax <= 2) return pickOccupancy<2, IP>(highOccupancy);
+  if (smax <= 3) return pickOccupancy<3, IP>(highOccupancy);
+  if (smax <= 4) return pickOccupancy<4, IP>(highOccupancy);
+  return pickOccupancy<8, IP>(highOccupancy);
+}
+
+KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax, bool ip, bool highOccupancy) {
+  return ip ? pickSlots<true>(smax, highOccupancy) : pickSlots<false>(smax, highOccupancy);
 }
 
 }  // namespace dev

@@ -35,6 +35,13 @@ constexpr int kWarpPhaseElems = 5 * kWarpPhaseTableMax;
 constexpr unsigned FULL = 0xffffffffu;
 // off-diagonal slots of the warp kernel's padded tables
 constexpr int kWarpSlots = 8;
+// Stage derivatives k1..k4 of the warp kernel live in shared memory (each lane touches only
+// its own rows, so no synchronisation) when a lane holds three or four rows: their registers
+// would otherwise cap the resident warps and spill.
+__host__ __device__ constexpr bool warpStagesInShared(int E) { return E >= 3; }
+// per-warp shared-memory vectors of DMAX elements: two stage-vector slabs, the step-back
+// cache, and k1..k4 when they are kept there
+__host__ __device__ constexpr int warpSmemVectors(int E) { return warpStagesInShared(E) ? 7 : 3; }
 
 // ---- complex helpers ---------------------------------------------------------
 template <typename R>
@@ -337,6 +344,8 @@ struct Worker {
   C2* buf0;
   C2* buf1;
   C2* cache;
+  C2* kst;  // k1..k4, each DMAX elements (warpStagesInShared(E))
+  static constexpr bool KSMEM = warpStagesInShared(E);
   WarpScratch* ws;
   double2* phs;  // per-warp phase region [5][kWarpPhaseTableMax] or null
   bool phsOn;    // this attempt's stage phases come from phs
@@ -365,7 +374,8 @@ struct Worker {
 
   __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w,
                                     double2* ph)
-      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), ws(w), phs(ph), phsOn(false), phsTab(false) {
+      : sysp(s), ra(a), lane(l), buf0(b0), buf1(b1), cache(c), kst(c + DMAX), ws(w), phs(ph), phsOn(false),
+        phsTab(false) {
     D = s->D;
     S = s->S;
     nJ = s->nJ;
@@ -475,13 +485,132 @@ struct Worker {
     }
   }
 
+  // The five further Cash-Karp stages of one attempt from k0 = (H/i) x, then the 5th-order
+  // solution (into y) and the rows' part of Odeint's error norm.  Both variants compute the
+  // same expressions in the same order (bit-identical): stagesRegisters keeps k1..k5 in
+  // registers, stagesShared keeps k1..k4 in the warp's shared memory, each lane reading back
+  // only the rows it wrote.
+  __device__ __forceinline__ void stagesRegisters(double dt, const C2 (&k0)[E], C2 (&y)[E], ErrNormMax& errLocal) {
+    C2 k1[E], k2[E], k3[E], k4[E], k5[E];
+    {
+      const R s0 = R(dt * CK::a10);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s0, k0[e], x[e]);
+    }
+    rhs(y, k1, t + CK::c1 * dt - t0, 1, buf1);
+    {
+      const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s1, k1[e], axpy(s0, k0[e], x[e]));
+    }
+    rhs(y, k2, t + CK::c2 * dt - t0, 2, buf0);
+    {
+      const R s0 = R(dt * CK::a30), s1 = R(dt * CK::a31), s2 = R(dt * CK::a32);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])));
+    }
+    rhs(y, k3, t + CK::c3 * dt - t0, 3, buf1);
+    {
+      const R s0 = R(dt * CK::a40), s1 = R(dt * CK::a41), s2 = R(dt * CK::a42), s3 = R(dt * CK::a43);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e]))));
+    }
+    rhs(y, k4, t + CK::c4 * dt - t0, 4, buf0);
+    {
+      const R s0 = R(dt * CK::a50), s1 = R(dt * CK::a51), s2 = R(dt * CK::a52), s3 = R(dt * CK::a53),
+              s4 = R(dt * CK::a54);
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        y[e] = axpy(s4, k4[e], axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])))));
+    }
+    rhs(y, k5, t + CK::c5 * dt - t0, 5, buf1);
+    solutionAndError(dt, k0, k2, k3, k4, k5, y, errLocal);
+  }
+
+  __device__ __forceinline__ void stagesShared(double dt, const C2 (&k0)[E], C2 (&y)[E], ErrNormMax& errLocal) {
+    C2* const K1 = kst;
+    C2* const K2 = kst + DMAX;
+    C2* const K3 = kst + 2 * DMAX;
+    C2* const K4 = kst + 3 * DMAX;
+    C2 kc[E];
+    {
+      const R s0 = R(dt * CK::a10);
+#pragma unroll
+      for (int e = 0; e < E; ++e) y[e] = axpy(s0, k0[e], x[e]);
+    }
+    rhs(y, kc, t + CK::c1 * dt - t0, 1, buf1);
+    {
+      const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        K1[row(e)] = kc[e];
+        y[e] = axpy(s1, kc[e], axpy(s0, k0[e], x[e]));
+      }
+    }
+    rhs(y, kc, t + CK::c2 * dt - t0, 2, buf0);
+    {
+      const R s0 = R(dt * CK::a30), s1 = R(dt * CK::a31), s2 = R(dt * CK::a32);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        K2[row(e)] = kc[e];
+        y[e] = axpy(s2, kc[e], axpy(s1, K1[row(e)], axpy(s0, k0[e], x[e])));
+      }
+    }
+    rhs(y, kc, t + CK::c3 * dt - t0, 3, buf1);
+    {
+      const R s0 = R(dt * CK::a40), s1 = R(dt * CK::a41), s2 = R(dt * CK::a42), s3 = R(dt * CK::a43);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        K3[row(e)] = kc[e];
+        y[e] = axpy(s3, kc[e], axpy(s2, K2[row(e)], axpy(s1, K1[row(e)], axpy(s0, k0[e], x[e]))));
+      }
+    }
+    rhs(y, kc, t + CK::c4 * dt - t0, 4, buf0);
+    {
+      const R s0 = R(dt * CK::a50), s1 = R(dt * CK::a51), s2 = R(dt * CK::a52), s3 = R(dt * CK::a53),
+              s4 = R(dt * CK::a54);
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        K4[row(e)] = kc[e];
+        y[e] = axpy(s4, kc[e],
+                    axpy(s3, K3[row(e)], axpy(s2, K2[row(e)], axpy(s1, K1[row(e)], axpy(s0, k0[e], x[e])))));
+      }
+    }
+    rhs(y, kc, t + CK::c5 * dt - t0, 5, buf1);
+    C2 k2[E], k3[E], k4[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      k2[e] = K2[row(e)];
+      k3[e] = K3[row(e)];
+      k4[e] = K4[row(e)];
+    }
+    solutionAndError(dt, k0, k2, k3, k4, kc, y, errLocal);
+  }
+
+  // 5th-order solution into y, embedded error and the rows' part of the Odeint error norm
+  __device__ __forceinline__ void solutionAndError(double dt, const C2 (&k0)[E], const C2 (&k2)[E], const C2 (&k3)[E],
+                                                   const C2 (&k4)[E], const C2 (&k5)[E], C2 (&y)[E],
+                                                   ErrNormMax& errLocal) {
+    const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
+    const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4), e5 = R(dt * CK::e5);
+    const double adt = fabs(dt);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      y[e] = axpy(b5, k5[e], axpy(b3, k3[e], axpy(b2, k2[e], axpy(b0, k0[e], x[e]))));
+      C2 xe = mk<C2>(0, 0);
+      xe = axpy(e5, k5[e], axpy(e4, k4[e], axpy(e3, k3[e], axpy(e2, k2[e], axpy(e0, k0[e], xe)))));
+      // a padding row (all zero) never raises the maximum
+      errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(x[e]) + adt * cabs(k0[e])));
+    }
+  }
+
   // one adaptive ODE step towards at most deltaT (ode_engine::Base::step, ODE.h:234-262,
   // with Boost.Odeint's controlled_runge_kutta<runge_kutta_cash_karp54>::try_step)
   __device__ __forceinline__ bool odeStep(double deltaT) {
     const double timeBefore = t;
     const double nextDtTry = fabs(deltaT) < fabs(dtTry / 10.) ? dtTry : 0.;
     if (fabs(dtTry) > fabs(deltaT)) dtTry = deltaT;
-    C2 k0[E], k1[E], k2[E], k3[E], k4[E], k5[E], y[E];
+    C2 k0[E], y[E];
     // dxdt at the start is the same for every attempt (Odeint recomputes it per try)
     rhs(x, k0, t - t0, 0, buf0);
     for (int attempt = 0;; ++attempt) {
@@ -495,53 +624,11 @@ struct Worker {
         phsOn = phsTab && hasFreq && t == t0;
         if (phsOn) preparePhases(dt);
       }
-      {
-        const R s0 = R(dt * CK::a10);
-#pragma unroll
-        for (int e = 0; e < E; ++e) y[e] = axpy(s0, k0[e], x[e]);
-      }
-      rhs(y, k1, t + CK::c1 * dt - t0, 1, buf1);
-      {
-        const R s0 = R(dt * CK::a20), s1 = R(dt * CK::a21);
-#pragma unroll
-        for (int e = 0; e < E; ++e) y[e] = axpy(s1, k1[e], axpy(s0, k0[e], x[e]));
-      }
-      rhs(y, k2, t + CK::c2 * dt - t0, 2, buf0);
-      {
-        const R s0 = R(dt * CK::a30), s1 = R(dt * CK::a31), s2 = R(dt * CK::a32);
-#pragma unroll
-        for (int e = 0; e < E; ++e) y[e] = axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])));
-      }
-      rhs(y, k3, t + CK::c3 * dt - t0, 3, buf1);
-      {
-        const R s0 = R(dt * CK::a40), s1 = R(dt * CK::a41), s2 = R(dt * CK::a42), s3 = R(dt * CK::a43);
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-          y[e] = axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e]))));
-      }
-      rhs(y, k4, t + CK::c4 * dt - t0, 4, buf0);
-      {
-        const R s0 = R(dt * CK::a50), s1 = R(dt * CK::a51), s2 = R(dt * CK::a52), s3 = R(dt * CK::a53),
-                s4 = R(dt * CK::a54);
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-          y[e] = axpy(s4, k4[e], axpy(s3, k3[e], axpy(s2, k2[e], axpy(s1, k1[e], axpy(s0, k0[e], x[e])))));
-      }
-      rhs(y, k5, t + CK::c5 * dt - t0, 5, buf1);
-      // 5th-order solution, embedded error and the Odeint error norm (max over rows)
-      const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
-      const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
-              e5 = R(dt * CK::e5);
-      const double adt = fabs(dt);
       ErrNormMax errLocal;
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        y[e] = axpy(b5, k5[e], axpy(b3, k3[e], axpy(b2, k2[e], axpy(b0, k0[e], x[e]))));
-        C2 xe = mk<C2>(0, 0);
-        xe = axpy(e5, k5[e], axpy(e4, k4[e], axpy(e3, k3[e], axpy(e2, k2[e], axpy(e0, k0[e], xe)))));
-        // a padding row (all zero) never raises the maximum
-        errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(x[e]) + adt * cabs(k0[e])));
-      }
+      if constexpr (KSMEM)
+        stagesShared(dt, k0, y, errLocal);
+      else
+        stagesRegisters(dt, k0, y, errLocal);
       double err = warpMax(errLocal.value());
       if (!(err == err)) {  // NaN error norm
         status |= 1u;
@@ -879,26 +966,37 @@ struct Worker {
 // CTAs of 128 threads the compiler must fit on one SM.  Three (at most 170 registers per
 // thread, some spills) for the Schroedinger-picture instance with three rows per lane, where
 // the 12 resident warps hide more latency than the spills cost (qubit-mode 2x40: FP64 113.0
-// -> 117.8 M steps/s, FP32 122.7 -> 141.2 M); one (255 registers, 8 warps) elsewhere, where
-// three or four measured slower (pumped lossy mode E = 1: -1 % / -12 %; interaction-picture
-// E = 3: -6 % / -14 %).
+// -> 117.8 M steps/s, FP32 122.7 -> 141.2 M, with the stage derivatives in registers); one
+// (255 registers, 8 warps) elsewhere, where three or four measured slower (pumped lossy mode
+// E = 1: -1 % / -12 %; interaction-picture E = 3: -6 % / -14 %).
 template <int E, bool IP>
 struct WarpMinBlocks {
   static constexpr int value = (!IP && E == 3) ? 3 : 1;
 };
+// A second instance with more resident CTAs (fewer registers) for Schroedinger-picture groups
+// with three or four rows per lane and at most four slots, whose stage derivatives k1..k4 sit
+// in shared memory; the autotuner times both and keeps the faster.
+__host__ __device__ constexpr bool warpHighOccupancyVariant(int E, int SMAX, bool IP) {
+  return !IP && E >= 3 && SMAX <= 4;
+}
+template <int E>
+struct WarpMinBlocksHigh {
+  static constexpr int value = E == 3 ? 4 : 3;
+};
 
-template <typename R, int E, int SMAX, bool IP>
-__global__ void __launch_bounds__(128, (WarpMinBlocks<E, IP>::value)) mcwfWarpKernel(TrajDev td, RunArgs ra) {
+template <typename R, int E, int SMAX, bool IP, int MINB>
+__global__ void __launch_bounds__(128, MINB) mcwfWarpKernel(TrajDev td, RunArgs ra) {
   using C2 = typename CT<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int DMAX = 32 * E;
-  C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * 3 * DMAX;
+  constexpr int NV = warpSmemVectors(E);
+  C2* base = reinterpret_cast<C2*>(smem) + size_t(warp) * NV * DMAX;
   WarpScratch* ws =
-      reinterpret_cast<WarpScratch*>(smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) + warp;
+      reinterpret_cast<WarpScratch*>(smem + size_t(blockDim.x / 32) * NV * DMAX * sizeof(C2)) + warp;
   // optional phase tables after every warp's scratch: [warps][kWarpPhaseElems] double2
   double2* phs = IP && ra.phaseCache ? reinterpret_cast<double2*>(reinterpret_cast<WarpScratch*>(
-                                     smem + size_t(blockDim.x / 32) * 3 * DMAX * sizeof(C2)) +
+                                     smem + size_t(blockDim.x / 32) * NV * DMAX * sizeof(C2)) +
                                  blockDim.x / 32) +
                                      size_t(warp) * kWarpPhaseElems
                                : nullptr;

@@ -152,7 +152,9 @@ typedef struct cqg_mcwf_pars {
                                   and 512 for CTA-per-trajectory groups */
   int32_t cta_shared_vectors;  /* with cta_threads > 0, for CTA-per-trajectory groups: 1 keeps
                                   the stage derivatives in shared memory (when they fit), 0 in
-                                  a global scratch slab; the autotuner chooses otherwise */
+                                  a global scratch slab; for warp-per-trajectory groups: 1 runs
+                                  the instance compiled for more resident CTAs per SM (where
+                                  there is one); the autotuner chooses otherwise */
   int32_t ip_phase_table;      /* interaction-picture phases exp(tau f) of the off-diagonal
                                   terms: 0 forms them once per distinct frequency f of the
                                   system (at most 128 on the warp kernel: per attempt, the
@@ -270,7 +272,8 @@ int cqg_ensemble_last_kernel_ms(const cqg_ensemble* ens, double* kernel_ms, doub
  * one persistent launch per run call, the groups on concurrent streams.  Writes the number
  * of groups to *n_groups and, for the first min(n_groups, cap) groups, five int32 each to
  * plan: kind (0 = warp per trajectory, 1 = CTA per trajectory with the stage derivatives in
- * global scratch, 2 = CTA per trajectory with them in shared memory), rows per lane E (warp
+ * global scratch, 2 = CTA per trajectory with them in shared memory, 3 = warp per trajectory
+ * with the instance compiled for more resident CTAs per SM), rows per lane E (warp
  * kind), off-diagonal slot bound, CTA threads, trajectories in the group. */
 int cqg_ensemble_plan(const cqg_ensemble* ens, int32_t* n_groups, int32_t* plan, int32_t cap);
 

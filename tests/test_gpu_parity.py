@@ -446,6 +446,28 @@ def test_cta_shape_does_not_change_warp_trajectories(gpu):
     assert np.array_equal(states[0], states[1]) and np.array_equal(states[0], states[2])
 
 
+def test_warp_kernel_occupancy_instances_agree(gpu):
+    """The qubit-mode system (three rows per lane) on the default instance and on the one
+    compiled for more resident CTAs per SM, each at 64 and 128 threads: the same arithmetic,
+    so bit-identical states, times and counters."""
+    model = gpu.Model("QbitMode_C++QED", C2_ARGS)
+    sysd = gpu.System(model.desc)
+    n = 600
+    out = []
+    for cta, high in ((128, 0), (64, 1), (128, 1)):
+        pars = model.run_pars().mcwf
+        pars.autotune = 0
+        pars.cta_threads = cta
+        pars.cta_shared_vectors = high
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        plan = ens.plan()
+        assert len(plan) == 1 and plan[0]["kind"] == (3 if high else 0) and plan[0]["threads"] == cta
+        ens.run(0.5, 2)
+        out.append((np.stack([ens.state(i, model.dim) for i in range(0, n, 37)]), ens.times()[0], ens.counters()))
+    for st, t, c in out[1:]:
+        assert np.array_equal(st, out[0][0]) and np.array_equal(t, out[0][1]) and np.array_equal(c, out[0][2])
+
+
 def test_block_kernel_cta_shapes_agree(gpu):
     """The CTA-per-trajectory kernel with 64, 160, 256 and 512 threads (one to eight rows per
     thread at D = 450) follows the same trajectories up to the summation order."""
