@@ -837,7 +837,7 @@ def main():
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": "f64" if args.precision == "fp64" else "f32-state/f64-control", "data": "synthetic",
-               "config": dict(workload_config(args, world), kernel_groups=r["plan"]),
+               "config": workload_config(args, world), "kernel_groups": r["plan"],
                "e2e": r["e2e"], "roofline": r["roofline"], "apply_roofline": r["apply"], "cpu_baseline": cpu,
                "clocks": r["clocks"],
                "gpu_launches": 3 * args.steps,
