@@ -129,6 +129,11 @@ def parse():
     ap.add_argument("--rng", default="pcg64", choices=["pcg64", "philox"])
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cta-threads", type=int, default=0,
+                    help="force this CTA size on every kernel group (no autotuning)")
+    ap.add_argument("--cta-shared-vectors", type=int, default=0,
+                    help="with --cta-threads: 1 selects the shared-memory stage vectors (CTA kernel) or the "
+                         "high-occupancy instance (warp kernel)")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave out the batched-vs-plain, accuracy and serving checks of the default line")
     ap.add_argument("--apply-states", type=int, default=0,
@@ -299,6 +304,10 @@ def run_ours(args, rank, world, dev):
     pars.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
     pars.precision = A.FP64 if args.precision == "fp64" else A.FP32
     pars.prng_stream = sharding.first_stream(1, n_traj, rank)
+    if args.cta_threads:
+        pars.autotune = 0
+        pars.cta_threads = args.cta_threads
+        pars.cta_shared_vectors = args.cta_shared_vectors
     system = cqg.System(model.desc)
     psi0 = model.initial_state()
     ens = cqg.Ensemble(system, psi0, n_traj, pars)

@@ -794,7 +794,8 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       const int shape = tunedThreads(*e, gi, systems, nSys, psi0s, psi0Off, *pars);
       e->groups[gi].threads = shape & 0xffff;
       e->groups[gi].smemVectors = (shape & (1 << 16)) != 0;
-      e->groups[gi].highOccupancy = (shape & kHighOccupancyFlag) != 0;
+      e->groups[gi].highOccupancy = (shape & kHighOccupancyFlag) != 0 && e->groups[gi].kind == 0 &&
+                                    !e->groups[gi].anyFreq;
     }
   *out = e.release();
   return CQG_OK;
@@ -993,9 +994,9 @@ bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device) {
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,
                  const cqg_complex* psi0s, const int64_t* psi0Off, const cqg_mcwf_pars& pars) {
   static std::mutex mu;
-  static std::map<std::tuple<int, int, int, int, int, int>, int> cache;
+  static std::map<std::tuple<int, int, int, int, int, int, bool>, int> cache;
   const KernelGroup& g = e.groups[gi];
-  const auto key = std::make_tuple(e.device, pars.precision, g.kind, g.E, g.smax, g.Dmax);
+  const auto key = std::make_tuple(e.device, pars.precision, g.kind, g.E, g.smax, g.Dmax, g.anyFreq);
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
@@ -1004,9 +1005,10 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   const std::vector<int> cands = threadCandidates(g, sharedVectorsFit(g, e.elemBytes, e.device));
   int nSM = 0;
   ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e.device), "attribute");
-  // enough trajectories to fill the device a couple of times over
-  const int64_t want = g.kind ? int64_t(nSM) * 4 : int64_t(nSM) * 16;
-  if (g.count < want / 2) return defaultThreads(g);  // too small to time; nothing cached
+  // the group itself up to a few fills of the device: the number of waves the resident CTAs
+  // take decides as much as their speed, so the sample has the group's own count where it can
+  const int64_t want = g.kind ? int64_t(nSM) * 16 : int64_t(nSM) * 64;
+  if (g.count < (g.kind ? int64_t(nSM) * 2 : int64_t(nSM) * 8)) return defaultThreads(g);  // too small to time
   const int64_t n = std::min<int64_t>(g.count, want);
   std::vector<int> order(e.nTraj);
   ck(cudaMemcpy(order.data(), e.dOrder, order.size() * sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy(order)");
@@ -1032,17 +1034,23 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   ra.T = 1e300;
   int best = defaultThreads(g);
   float bestMs = 0;
-  for (int pass = 0; pass < 2; ++pass)  // pass 0 warms up every candidate
-    for (int c : cands) {
+  // pass 0 warms up every candidate (and moves the sample away from its initial state);
+  // passes 1 and 2 time each candidate over 48 MCWF steps and keep its faster time
+  std::vector<float> ms(cands.size(), 0.f);
+  for (int pass = 0; pass < 3; ++pass)
+    for (size_t ci = 0; ci < cands.size(); ++ci) {
+      const int c = cands[ci];
       tmp->groups[0].threads = c & 0xffff;
       tmp->groups[0].smemVectors = (c & (1 << 16)) != 0;
       tmp->groups[0].highOccupancy = (c & kHighOccupancyFlag) != 0;
-      ra.nSteps = pass ? 12 : 2;
+      ra.nSteps = pass ? 48 : 8;
       if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
-      if (pass && (bestMs == 0 || tmp->lastMs < bestMs)) {
-        bestMs = tmp->lastMs;
-        best = c;
-      }
+      if (pass) ms[ci] = pass == 1 ? tmp->lastMs : std::min(ms[ci], tmp->lastMs);
+    }
+  for (size_t ci = 0; ci < cands.size(); ++ci)
+    if (bestMs == 0 || ms[ci] < bestMs) {
+      bestMs = ms[ci];
+      best = cands[ci];
     }
   std::lock_guard<std::mutex> lock(mu);
   cache[key] = best;

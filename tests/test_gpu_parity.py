@@ -438,7 +438,8 @@ def test_cta_shape_does_not_change_warp_trajectories(gpu):
         pars.cta_threads = cta
         ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
         plan = ens.plan()
-        assert len(plan) == 1 and plan[0]["kind"] == 0 and plan[0]["threads"] in (64, 128)
+        # kind 3: the instance compiled for more resident CTAs, which the autotuner may choose
+        assert len(plan) == 1 and plan[0]["kind"] in (0, 3) and plan[0]["threads"] in (64, 128)
         if cta:
             assert plan[0]["threads"] == cta
         ens.run(0.2, 1)
