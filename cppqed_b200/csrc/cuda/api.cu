@@ -1034,18 +1034,37 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
   ra.T = 1e300;
   int best = defaultThreads(g);
   float bestMs = 0;
-  // pass 0 warms up every candidate (and moves the sample away from its initial state);
-  // passes 1 and 2 time each candidate over 48 MCWF steps and keep its faster time
+  auto setShape = [&](int c) {
+    tmp->groups[0].threads = c & 0xffff;
+    tmp->groups[0].smemVectors = (c & (1 << 16)) != 0;
+    tmp->groups[0].highOccupancy = (c & kHighOccupancyFlag) != 0;
+  };
+  // Warm-up: every candidate advances the sample by 8 MCWF steps (which also moves it away
+  // from its initial state).  The candidates are then timed as the ensemble runs: every
+  // trajectory advanced over the same interval of simulated time (a varying number of steps
+  // each, the interval sized for about 48 steps), twice, keeping each candidate's faster time.
+  for (int c : cands) {
+    setShape(c);
+    ra.nSteps = 8;
+    if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
+  }
+  std::vector<double> tt(size_t(tmp->nTraj));
+  ck(cudaMemcpy(tt.data(), tmp->td.t, tt.size() * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy(times)");
+  double tNow = *std::max_element(tt.begin(), tt.end());
+  const double interval = tNow / (8. * double(cands.size())) * 48.;
   std::vector<float> ms(cands.size(), 0.f);
-  for (int pass = 0; pass < 3; ++pass)
+  for (int pass = 1; pass <= 2; ++pass)
     for (size_t ci = 0; ci < cands.size(); ++ci) {
-      const int c = cands[ci];
-      tmp->groups[0].threads = c & 0xffff;
-      tmp->groups[0].smemVectors = (c & (1 << 16)) != 0;
-      tmp->groups[0].highOccupancy = (c & kHighOccupancyFlag) != 0;
-      ra.nSteps = pass ? 48 : 8;
+      setShape(cands[ci]);
+      if (interval > 0 && std::isfinite(interval)) {
+        ra.mode = dev::RUN_TO;
+        ra.tEnd = tNow + interval;
+        tNow = ra.tEnd;
+      } else {
+        ra.nSteps = 48;
+      }
       if (launchRun(tmp, ra, 0, nullptr) != CQG_OK) return defaultThreads(g);
-      if (pass) ms[ci] = pass == 1 ? tmp->lastMs : std::min(ms[ci], tmp->lastMs);
+      ms[ci] = pass == 1 ? tmp->lastMs : std::min(ms[ci], tmp->lastMs);
     }
   for (size_t ci = 0; ci < cands.size(); ++ci)
     if (bestMs == 0 || ms[ci] < bestMs) {
