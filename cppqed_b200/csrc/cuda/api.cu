@@ -372,49 +372,6 @@ void buildSystemDevice(cqg_system& s) {
         for (int64_t r = 0; r < D; ++r) wfIdx[k * Dp + r] = fIdx[k * D + r];
     }
   }
-  // The per-axis Hamiltonian for the CTA kernel: slot descriptors, factors and frequencies,
-  // and the multi-index of a row by multiply-high divisions, checked on every row here.
-  std::vector<dev::FacSlot> fslots;
-  std::vector<dcomp> facVals, facFreqs;
-  int fRank = 0, fN[3] = {1, 1, 1};
-  unsigned fMagic[3] = {0, 0, 0};
-  if (L.fac.ok && L.rank <= 3 && L.fac.slots.size() <= size_t(dev::kMaxFacSlots)) {
-    fRank = L.rank;
-    for (int a = 0; a < fRank; ++a) {
-      fN[a] = int(L.dims[a]);
-      fMagic[a] = fN[a] > 1 ? unsigned(((uint64_t(1) << 32) + uint64_t(fN[a]) - 1) / uint64_t(fN[a])) : 0u;
-    }
-    bool exact = true;
-    for (int64_t r = 0; r < D && exact; ++r) {
-      uint64_t q = uint64_t(r), rem = uint64_t(r);
-      for (int a = fRank - 1; a >= 0; --a) {
-        const uint64_t qq = fN[a] > 1 ? (q * fMagic[a]) >> 32 : q;
-        const uint64_t i = q - qq * uint64_t(fN[a]);
-        if (qq != rem / uint64_t(fN[a]) || i != rem % uint64_t(fN[a])) exact = false;
-        q = qq;
-        rem /= uint64_t(fN[a]);
-      }
-    }
-    if (exact) {
-      for (const auto& f : L.fac.slots) {
-        dev::FacSlot d{};
-        d.nAx = f.nAx;
-        for (int a = 0; a < f.nAx; ++a) {
-          d.axis[a] = f.axis[a];
-          d.digit[a] = f.digit[a];
-          d.K[a] = int(f.K[a]);
-          d.N[a] = int(L.dims[f.axis[a]]);
-          d.off[a] = f.off[a];
-        }
-        d.inShift = int(f.inShift);
-        fslots.push_back(d);
-      }
-      facVals = L.fac.factors;
-      if (L.fac.anyFreq) facFreqs = L.fac.freqs;
-    }
-  }
-  const size_t oFslot = A.add(fslots.size() * sizeof(dev::FacSlot) + 16), oFacD = A.add(facVals.size() * 16 + 16),
-               oFacF = A.add(facVals.size() * 8 + 8), oFacFr = A.add(facFreqs.size() * 16 + 16);
   const size_t oWcol = A.add(wcol.size() * 4 + 4), oWdiagD = A.add(wdiag.size() * 16 + 16),
                oWvalD = A.add(wval.size() * 16 + 16), oWdiagF = A.add(wdiag.size() * 8 + 8),
                oWvalF = A.add(wval.size() * 8 + 8), oWjw = A.add(wjw.size() * 8 + 8),
@@ -461,10 +418,6 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oWlambda, toD2(wlambda));
   upload(b, oWfIdx, wfIdx);
   upload(b, oWfreq, toD2(wfreq));
-  upload(b, oFslot, fslots);
-  upload(b, oFacD, toD2(facVals));
-  upload(b, oFacF, toF2(facVals));
-  upload(b, oFacFr, toD2(facFreqs));
   auto& sd = s.sd;
   sd.D = int(D);
   sd.S = S;
@@ -504,20 +457,6 @@ void buildSystemDevice(cqg_system& s) {
   sd.diagF = reinterpret_cast<const float2*>(b + oDiagF);
   sd.valF = reinterpret_cast<const float2*>(b + oValF);
   sd.jvalF = reinterpret_cast<const float2*>(b + oJvalF);
-  sd.diagZero = 1;
-  for (const auto& v : H.diag)
-    if (v != dcomp(0, 0)) sd.diagZero = 0;
-  sd.nFS = int(fslots.size());
-  sd.nFac = int(facVals.size());
-  sd.facRank = fRank;
-  for (int a = 0; a < 3; ++a) {
-    sd.facN[a] = fN[a];
-    sd.facMagic[a] = fMagic[a];
-  }
-  sd.fslot = fslots.empty() ? nullptr : reinterpret_cast<const dev::FacSlot*>(b + oFslot);
-  sd.facD = fslots.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFacD);
-  sd.facF = fslots.empty() ? nullptr : reinterpret_cast<const float2*>(b + oFacF);
-  sd.facFr = facFreqs.empty() ? nullptr : reinterpret_cast<const double2*>(b + oFacFr);
   sd.Dp = warpTables ? int(Dp) : 0;
   sd.wcol = warpTables ? reinterpret_cast<const int*>(b + oWcol) : nullptr;
   sd.wdiagD = warpTables ? reinterpret_cast<const double2*>(b + oWdiagD) : nullptr;
@@ -830,7 +769,6 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
       g.smax = std::max(g.smax, s->sd.S);
       g.anyFreq |= s->sd.hasFreq != 0;
       g.phaseElems = std::max(g.phaseElems, blockPhaseElems(s->sd));
-      g.facElems = std::max(g.facElems, blockFacElems(s->sd));
     }
     g.count = k - g.first;
     e->groups.push_back(g);
@@ -849,7 +787,7 @@ int createEnsemble(const cqg_system* const* systems, int nSys, const int32_t* sy
                       dev::warpHighOccupancyVariant(g.E, g.smax <= 2 ? 2 : g.smax <= 3 ? 3 : g.smax <= 4 ? 4 : 8,
                                                     g.anyFreq);
     g.phaseTable = pars->ip_phase_table >= 0;
-    if (!g.phaseTable || g.kind == 0) g.phaseElems = g.facElems = 0;
+    if (!g.phaseTable || g.kind == 0) g.phaseElems = 0;
   }
   if (pars->autotune && pars->cta_threads <= 0)
     for (size_t gi = 0; gi < e->groups.size(); ++gi) {
@@ -898,15 +836,9 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
       int device = 0, optin = 0;
       ck(cudaGetDevice(&device), "cudaGetDevice");
       ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
-      if (blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems, g.facElems) > size_t(optin)) g.phaseElems = 0;
+      if (blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems) > size_t(optin)) g.phaseElems = 0;
     }
-    if (g.facElems > 0) {  // per-axis factors that do not fit leave the trajectories on the ELL tables
-      int device = 0, optin = 0;
-      ck(cudaGetDevice(&device), "cudaGetDevice");
-      ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
-      if (blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems, g.facElems) > size_t(optin)) g.facElems = 0;
-    }
-    const size_t smem = blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems, g.facElems);
+    const size_t smem = blockSmemBytes(g.Dmax, elemBytes, g.smemVectors, g.phaseElems);
     ck(cudaFuncSetAttribute(reinterpret_cast<const void*>(fn), cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
        "cudaFuncSetAttribute");
     int perSM = 0;
@@ -918,7 +850,6 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
     bsc.stride = (g.Dmax + 31) / 32 * 32;
     bsc.base = nullptr;
     bsc.phaseElems = g.phaseElems;
-    bsc.facElems = g.facElems;
     if (!g.smemVectors) {
       const size_t need = size_t(grid) * dev::kBlockVectors * size_t(bsc.stride) * elemBytes;
       if (need > g.scratchBytes) {
@@ -1057,7 +988,7 @@ std::vector<int> threadCandidates(const KernelGroup& g, bool vectorsFit) {
 bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device) {
   int optin = 0;
   ck(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attribute");
-  return g.kind == 1 && blockSmemBytes(g.Dmax, elemBytes, true, g.phaseElems, g.facElems) <= size_t(optin);
+  return g.kind == 1 && blockSmemBytes(g.Dmax, elemBytes, true, g.phaseElems) <= size_t(optin);
 }
 
 int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* systems, int nSys,

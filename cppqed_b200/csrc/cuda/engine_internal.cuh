@@ -85,8 +85,6 @@ struct KernelGroup {
   bool phaseTable = true;    // interaction picture: phases from the systems' tables of
                              // distinct frequencies where they have one
   int phaseElems = 0;        // CTA kind: shared-memory phase table capacity (max over systems)
-  int facElems = 0;          // CTA kind: shared-memory per-axis operator capacity (max over
-                             // systems; 0: every trajectory reads the ELL tables)
   int threads = 0;  // CTA size
   int64_t first = 0, count = 0;
   cudaStream_t stream = nullptr;
@@ -99,18 +97,15 @@ inline int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
 
 // Dynamic shared memory of the CTA kernel: two stage vectors of Dmax elements, the reduction
 // scratch and broadcast words, the interaction-picture phase table of phaseElems double2,
-// the per-axis operator of facElems entries, and with shared-memory vectors the kBlockVectors stage derivatives / candidate / cache of
+// and with shared-memory vectors the kBlockVectors stage derivatives / candidate / cache of
 // ceil32(Dmax) elements each.
-inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors, int phaseElems, int facElems) {
+inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors, int phaseElems) {
   const size_t base = 2 * size_t(Dmax) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64 +
-                      size_t(phaseElems) * sizeof(double2) + dev::blockFacBytes(facElems, elemBytes);
+                      size_t(phaseElems) * sizeof(double2);
   return base + (vectors ? size_t(dev::kBlockVectors) * size_t((Dmax + 31) / 32 * 32) * elemBytes : 0);
 }
-// Shared-memory capacities a CTA-kernel group needs for one of its systems (with the phase
-// tables on, ip_phase_table >= 0): the per-axis operator where the system has one, else the
-// table of its distinct interaction-picture frequencies
-inline int blockFacElems(const dev::SysDev& sd) { return sd.nFS > 0 ? sd.nFac : 0; }
-inline int blockPhaseElems(const dev::SysDev& sd) { return sd.hasFreq && sd.fIdx && sd.nFS == 0 ? sd.nFD : 0; }
+// Phase-table capacity a CTA-kernel group needs for one of its systems
+inline int blockPhaseElems(const dev::SysDev& sd) { return sd.hasFreq && sd.fIdx ? sd.nFD : 0; }
 
 // One persistent launch of group g over td on stream st (ra.order / nTasks / queue set by
 // the caller); allocates or grows the group's block-kernel scratch.

@@ -32,16 +32,7 @@ struct BlockScratch {
                         // follow the broadcast words in dynamic shared memory
   long long stride;     // elements per vector (>= max D)
   int phaseElems;       // IP: capacity of the shared-memory phase table (0: none)
-  int facElems;         // capacity of the shared-memory per-axis factors (0: the ELL tables)
 };
-
-// bytes of the shared-memory region of the per-axis operator: per factor entry its phase
-// (double2) and value, and the slot descriptors
-__host__ __device__ inline size_t blockFacBytes(int facElems, size_t elemBytes) {
-  if (facElems <= 0) return 0;
-  const size_t n = size_t((facElems + 1) / 2 * 2);  // keeps what follows 16-byte aligned
-  return n * (sizeof(double2) + elemBytes) + size_t(kMaxFacSlots) * sizeof(FacSlot);
-}
 
 // block-wide sums of n <= N uniform values; red holds 32 * N doubles of shared memory
 template <int N>
@@ -89,15 +80,6 @@ struct BlockWorker {
   const double2* fDist;
   int nFD;
   double2* phTab;  // IP: shared-memory phases of the distinct frequencies, or null
-  // the per-axis operator (SysDev::fslot ...) staged in shared memory, or nFS = 0
-  int nFS = 0, fRank = 0;
-  int fN[3];
-  unsigned fMagic[3];
-  const FacSlot* fsl;
-  const C2* fv;
-  double2* fph;         // IP: exp(tau f) per factor entry
-  const double2* facFr; // the entries' frequencies (device memory), or null
-  bool diagZero;        // no main-diagonal contribution
   C2* x;       // the trajectory's state (device memory)
   C2* vec;     // this CTA's scratch vectors
   long long stride;
@@ -116,75 +98,9 @@ struct BlockWorker {
   __device__ __forceinline__ C2* xnew() const { return vec + 6 * stride; }
   __device__ __forceinline__ C2* cache() const { return vec + 7 * stride; }
 
-  // out = (H/i) y from the per-axis operator: a row's coefficients are products of one
-  // shared-memory factor per retained axis (and, in the interaction picture, of the factors'
-  // phases exp(tau f), formed once per factor entry and right-hand side), so no table is
-  // read per row but the fused main diagonal
-  __device__ __forceinline__ void rhsFactored(const C2* ys, C2* out, double tau) {
-    bool phOn = false;
-    if constexpr (IP) {
-      phOn = facFr && tau != 0.;
-      if (phOn) {
-        __syncthreads();
-        for (int k = threadIdx.x; k < nFac(); k += blockDim.x) {
-          const double2 f = __ldg(&facFr[k]);
-          fph[k] = (f.x != 0. || f.y != 0.) ? cexpScaled(tau, f) : make_double2(1., 0.);
-        }
-        __syncthreads();
-      }
-    }
-    for (int r = threadIdx.x; r < D; r += blockDim.x) {
-      int idx[3] = {0, 0, 0};
-      unsigned q = unsigned(r);
-#pragma unroll
-      for (int a = 2; a >= 0; --a)
-        if (a < fRank) {
-          const unsigned qq = fMagic[a] ? __umulhi(q, fMagic[a]) : q;
-          idx[a] = int(q - qq * unsigned(fN[a]));
-          q = qq;
-        }
-      C2 acc = diagZero ? mk<C2>(0, 0) : cmul(diag[r], ys[r]);
-      for (int s = 0; s < nFS; ++s) {
-        const FacSlot& f = fsl[s];
-        bool ok = true;
-        int m[2] = {0, 0};
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-          if (a < f.nAx) {
-            const int ax = f.axis[a];
-            const int i = ax == 0 ? idx[0] : ax == 1 ? idx[1] : idx[2];
-            const int K = f.K[a];
-            if (f.digit[a] == 1) {
-              ok &= i >= K;
-              m[a] = i - K;
-            } else {
-              if (f.digit[a] == 2) ok &= i < f.N[a] - K;
-              m[a] = i;
-            }
-          }
-        if (!ok) continue;
-        C2 c = fv[f.off[0] + m[0]];
-        double2 ph = make_double2(1., 0.);
-        if (phOn) ph = fph[f.off[0] + m[0]];
-        if (f.nAx == 2) {
-          c = cmul(c, fv[f.off[1] + m[1]]);
-          if (phOn) ph = cmulD(ph, fph[f.off[1] + m[1]]);
-        }
-        if (phOn) c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
-        acc = cfma(c, ys[r + f.inShift], acc);
-      }
-      out[r] = acc;
-    }
-  }
-  __device__ __forceinline__ int nFac() const { return sysp->nFac; }
-
   // out = (H/i) y at picture time tau, y in shared memory
   __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
     ++nRhs;
-    if (nFS) {
-      rhsFactored(ys, out, tau);
-      return;
-    }
     bool tab = false;
     if constexpr (IP) {
       // exp(tau f) once per distinct frequency into shared memory: the same values, bit for
@@ -668,29 +584,8 @@ __global__ void __launch_bounds__(512, 1) mcwfBlockKernel(TrajDev td, RunArgs ra
     w.fDist = s->fDist;
     w.nFD = s->nFD;
     w.phTab = IP && s->fIdx && s->nFD <= bsc.phaseElems ? phTab : nullptr;
-    // then the per-axis operator: phases, slot descriptors, factor values
-    double2* facPh = phTab + bsc.phaseElems;
-    FacSlot* facSl = reinterpret_cast<FacSlot*>(facPh + (bsc.facElems + 1) / 2 * 2);
-    C2* facVal = reinterpret_cast<C2*>(facSl + kMaxFacSlots);
-    unsigned char* afterFac = reinterpret_cast<unsigned char*>(facPh) + blockFacBytes(bsc.facElems, sizeof(C2));
-    w.diagZero = s->diagZero != 0;
-    if (s->nFS > 0 && s->nFS <= kMaxFacSlots && s->nFac <= bsc.facElems) {
-      for (int k = threadIdx.x; k < s->nFS; k += blockDim.x) facSl[k] = s->fslot[k];
-      const C2* fg = Tables<R>::fac(*s);
-      for (int k = threadIdx.x; k < s->nFac; k += blockDim.x) facVal[k] = fg[k];
-      w.nFS = s->nFS;
-      w.fRank = s->facRank;
-      for (int a = 0; a < 3; ++a) {
-        w.fN[a] = s->facN[a];
-        w.fMagic[a] = s->facMagic[a];
-      }
-      w.fsl = facSl;
-      w.fv = facVal;
-      w.fph = facPh;
-      w.facFr = s->facFr;
-    }
     w.vec = bsc.base ? reinterpret_cast<C2*>(bsc.base) + size_t(blockIdx.x) * kBlockVectors * bsc.stride
-                     : reinterpret_cast<C2*>(afterFac);
+                     : reinterpret_cast<C2*>(phTab + bsc.phaseElems);
     w.stride = bsc.stride;
     w.ys0 = ys0;
     w.ys1 = ys1;

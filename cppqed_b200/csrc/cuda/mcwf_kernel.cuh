@@ -193,23 +193,6 @@ __device__ __forceinline__ double warpMax(double v) {
 }
 
 // ---- device-side system tables (see lowering.hpp) -----------------------------------
-// One off-diagonal diagonal of a Hamiltonian term in per-axis form (FactoredSlot of the
-// lowering): for an output row with indices i on the retained axes the coefficient is
-// prod_a factor[off[a] + m_a] (m_a = i_a - K for a "minus" digit, i_a otherwise), the input
-// row is the output row + inShift, and the row takes part when every "minus" axis has
-// i_a >= K and every "plus" axis i_a < N - K.
-constexpr int kMaxFacSlots = 16;
-struct FacSlot {
-  int nAx;
-  int axis[2];
-  int digit[2];
-  int K[2];
-  int N[2];
-  int off[2];
-  int inShift;
-  int pad[2];
-};
-
 struct SysDev {
   int D, S, SJ, SO, nJ, nObs, nAvr;
   int hasH, hasEx, hasFreq;
@@ -247,18 +230,6 @@ struct SysDev {
   const double2* wlambda;      // [Dp] (Exact) or null
   const unsigned short* wfIdx; // [kWarpSlots][Dp] (IP with a table) or null
   const double2* wfreq;        // [kWarpSlots][Dp] (IP) or null
-  // The Hamiltonian's off-diagonal terms per axis (CTA kernel), or nFS = 0: nFS slots, nFac
-  // factor entries with their summed interaction-picture frequencies (or null), and the
-  // system's axes (at most 3) for the row's multi-index, divisions by N by multiply-high
-  // with facMagic (0 for an axis of length 1).
-  int nFS, nFac, facRank;
-  int diagZero;  // the fused main diagonal is zero (no per-row diagonal read)
-  int facN[3];
-  unsigned facMagic[3];
-  const FacSlot* fslot;
-  const double2* facD;
-  const float2* facF;
-  const double2* facFr;
   // precision-specific copies
   const double2* diagD;
   const double2* valD;
@@ -277,7 +248,6 @@ struct Tables<double> {
   __device__ static const double2* jval(const SysDev& s) { return s.jvalD; }
   __device__ static const double2* wdiag(const SysDev& s) { return s.wdiagD; }
   __device__ static const double2* wval(const SysDev& s) { return s.wvalD; }
-  __device__ static const double2* fac(const SysDev& s) { return s.facD; }
 };
 template <>
 struct Tables<float> {
@@ -286,7 +256,6 @@ struct Tables<float> {
   __device__ static const float2* jval(const SysDev& s) { return s.jvalF; }
   __device__ static const float2* wdiag(const SysDev& s) { return s.wdiagF; }
   __device__ static const float2* wval(const SysDev& s) { return s.wvalF; }
-  __device__ static const float2* fac(const SysDev& s) { return s.facF; }
 };
 
 struct TrajDev {

@@ -307,7 +307,6 @@ void advance(cqg_server& s) {
     g.smax = 0;
     g.anyFreq = false;
     g.phaseElems = 0;
-    g.facElems = 0;
     g.phaseTable = s.pars.mcwf.ip_phase_table >= 0;
     for (auto& p : v) {
       order.push_back(p.second);
@@ -317,10 +316,7 @@ void advance(cqg_server& s) {
       if (groupKey(req->sys->L.D, req->sys->sd.S) == key) {
         g.smax = std::max(g.smax, req->sys->sd.S);
         g.anyFreq |= req->sys->sd.hasFreq != 0;
-        if (g.kind == 1 && g.phaseTable) {
-          g.phaseElems = std::max(g.phaseElems, blockPhaseElems(req->sys->sd));
-          g.facElems = std::max(g.facElems, blockFacElems(req->sys->sd));
-        }
+        if (g.kind == 1 && g.phaseTable) g.phaseElems = std::max(g.phaseElems, blockPhaseElems(req->sys->sd));
       }
     launch.push_back(&g);
   }

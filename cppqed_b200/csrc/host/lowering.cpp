@@ -137,80 +137,6 @@ EllOperator lowerGeneric(const Shape& s, const cqg_tridiagonal* terms, int n, co
   return toEll(s.D, rows, nullptr, anyFreq);
 }
 
-// The off-diagonal diagonals of the Hamiltonian terms as per-axis factors (see
-// FactoredOperator).  A rank-2 diagonal is factorised about its largest entry p:
-// f1[m1] = box[p0, m1], f0[m0] = box[m0, p1] / box[p0, p1], and its frequencies additively,
-// g1[m1] = fr[p0, m1], g0[m0] = fr[m0, p1] - fr[p0, p1]; a diagonal whose reconstruction
-// misses the box by more than 1e-14 of its largest entry leaves the operator unfactored.
-FactoredOperator factorHamiltonian(const Shape& s, const cqg_tridiagonal* terms, int n) {
-  FactoredOperator F;
-  constexpr size_t kMaxFactoredSlots = 16, kMaxFactors = 8192;
-  if (s.rank > 3) return F;
-  for (int i = 0; i < n; ++i) {
-    const cqg_tridiagonal& t = terms[i];
-    if (t.rank < 1 || t.rank > 2) return F;
-    const size_t L = t.rank == 1 ? 3 : 9;
-    for (size_t j = 0; j < L; ++j) {
-      const cqg_complex* dj = t.diagonals[j];
-      if (!dj) continue;
-      int dig[2] = {int(j), 0};
-      if (t.rank == 2) dig[0] = int(j / 3), dig[1] = int(j % 3);
-      if (dig[0] == 0 && dig[1] == 0) continue;  // a main diagonal: fused into ham.diag
-      FactoredSlot fs;
-      fs.nAx = t.rank;
-      int64_t ext[2] = {1, 1};
-      for (int a = 0; a < t.rank; ++a) {
-        fs.axis[a] = t.axes[a];
-        fs.digit[a] = dig[a];
-        fs.K[a] = t.differences[a];
-        const int64_t N = s.dims[t.axes[a]];
-        ext[a] = dig[a] == 0 ? N : N - fs.K[a];
-        fs.inShift += (dig[a] == 1 ? -fs.K[a] : dig[a] == 2 ? fs.K[a] : 0) * s.strides[t.axes[a]];
-      }
-      const cqg_complex* fj = t.freqs ? t.freqs[j] : nullptr;
-      const int64_t n0 = ext[0], n1 = ext[1];
-      auto box = [&](int64_t m0, int64_t m1) { return dcomp(dj[m0 * n1 + m1].re, dj[m0 * n1 + m1].im); };
-      auto fbox = [&](int64_t m0, int64_t m1) {
-        return fj ? dcomp(fj[m0 * n1 + m1].re, fj[m0 * n1 + m1].im) : dcomp(0, 0);
-      };
-      std::vector<dcomp> f0(n0), f1(n1, dcomp(1, 0)), g0(n0, dcomp(0, 0)), g1(n1, dcomp(0, 0));
-      if (t.rank == 1) {
-        for (int64_t m = 0; m < n0; ++m) f0[m] = box(m, 0), g0[m] = fbox(m, 0);
-      } else {
-        int64_t p0 = 0, p1 = 0;
-        double big = 0, fbig = 0;
-        for (int64_t a = 0; a < n0; ++a)
-          for (int64_t b = 0; b < n1; ++b) {
-            if (std::abs(box(a, b)) > big) big = std::abs(box(a, b)), p0 = a, p1 = b;
-            fbig = std::max(fbig, std::abs(fbox(a, b)));
-          }
-        if (big == 0) continue;  // an all-zero diagonal adds nothing
-        const dcomp piv = box(p0, p1);
-        for (int64_t b = 0; b < n1; ++b) f1[b] = box(p0, b), g1[b] = fbox(p0, b);
-        for (int64_t a = 0; a < n0; ++a) f0[a] = box(a, p1) / piv, g0[a] = fbox(a, p1) - fbox(p0, p1);
-        for (int64_t a = 0; a < n0; ++a)
-          for (int64_t b = 0; b < n1; ++b) {
-            if (std::abs(f0[a] * f1[b] - box(a, b)) > 1e-14 * big) return FactoredOperator{};
-            if (std::abs(g0[a] + g1[b] - fbox(a, b)) > 1e-14 * std::max(1., fbig)) return FactoredOperator{};
-          }
-      }
-      fs.off[0] = int(F.factors.size());
-      F.factors.insert(F.factors.end(), f0.begin(), f0.end());
-      F.freqs.insert(F.freqs.end(), g0.begin(), g0.end());
-      if (t.rank == 2) {
-        fs.off[1] = int(F.factors.size());
-        F.factors.insert(F.factors.end(), f1.begin(), f1.end());
-        F.freqs.insert(F.freqs.end(), g1.begin(), g1.end());
-      }
-      if (fj) F.anyFreq = true;
-      F.slots.push_back(fs);
-      if (F.slots.size() > kMaxFactoredSlots || F.factors.size() > kMaxFactors) return FactoredOperator{};
-    }
-  }
-  F.ok = !F.slots.empty();
-  return F;
-}
-
 }  // namespace
 
 LoweredSystem lowerSystem(const cqg_system_desc& d) {
@@ -238,7 +164,6 @@ LoweredSystem lowerSystem(const cqg_system_desc& d) {
         }
       });
     L.ham = toEll(s.D, rows, &diag, anyFreq);
-    L.fac = factorHamiltonian(s, d.ham, d.n_ham);
   }
 
   // Exact part: lambda[row] = sum_a lambda_a[n_a]

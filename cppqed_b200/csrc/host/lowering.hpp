@@ -27,36 +27,12 @@ struct EllOperator {
   std::vector<std::complex<double>> freq;  // [S][D] or empty when time-independent
 };
 
-// The Hamiltonian's off-diagonal terms in the per-axis form of the reference's Tridiagonal
-// (Tridiagonal.tcc:220-263): every non-empty off-diagonal diagonal of a term of rank 1 or 2
-// is a direct product of one vector per retained axis (how the reference builds every
-// Tridiagonal of rank > 1, Tridiagonal.tcc:56-64), so a row's coefficient is the product of
-// one entry per axis and its frequency the sum.  Built only when every such diagonal
-// factorises to rounding (1e-14 relative), the system has at most 3 axes and the slot count
-// is small; the main diagonals stay fused into `ham.diag`.
-struct FactoredSlot {
-  int nAx = 0;         // retained axes: 1 or 2
-  int axis[2] = {};    // system axes
-  int digit[2] = {};   // 0 main, 1 "minus" (out n+K <- in n), 2 "plus" (out n <- in n+K)
-  int64_t K[2] = {};
-  int off[2] = {};     // offsets of the per-axis factors in `factors`
-  int64_t inShift = 0; // input row minus output row
-};
-struct FactoredOperator {
-  bool ok = false;
-  std::vector<FactoredSlot> slots;          // in the reference's term / diagonal order
-  std::vector<std::complex<double>> factors;
-  std::vector<std::complex<double>> freqs;  // per factor entry, summed over the axes (IP)
-  bool anyFreq = false;
-};
-
 struct LoweredSystem {
   int rank = 0;
   int64_t dims[CQG_MAX_RANK] = {};
   int64_t D = 0;
   bool hasH = false, hasEx = false, hasLi = false;
   EllOperator ham;                     // H/i with fused diagonal
-  FactoredOperator fac;                // the same off-diagonal terms per axis, where they factorise
   std::vector<std::complex<double>> lambda;  // [D] Exact exponent per row (empty: none)
   std::vector<EllOperator> jumps;      // J_m, slots include diagonal entries
   std::vector<std::vector<double>> weights;  // [m][D] closed-form rate weights (empty: ||J psi||^2)

@@ -469,49 +469,6 @@ def test_warp_kernel_occupancy_instances_agree(gpu):
         assert np.array_equal(st, out[0][0]) and np.array_equal(t, out[0][1]) and np.array_equal(c, out[0][2])
 
 
-FACTORED_CASES = [
-    ("1particle1mode", ["--1p1mconf", "2", "--vClass", "0", "--modeCav", "Cos", "--kCav", "1", "--Unot", "-1",
-                        "--eta", "5", "--kappa", "1", "--cutoff", "8", "--fin", "5"], 0.1),
-    ("Optomechanics", ["--picture", "Sch", "--cutoffOpt", "15", "--cutoffMech", "30", "--etaOpt", "2", "--kappaOpt",
-                       "1", "--deltaCOpt", "-1", "--kappaMech", "0.1", "--deltaCMech", "-2", "--u", "0.2"], 0.5),
-    ("Optomechanics", ["--picture", "IP", "--cutoffOpt", "20", "--cutoffMech", "60", "--kappaOpt", "1",
-                       "--etaOpt", "1", "--deltaCOpt", "-1", "--deltaCMech", "-2", "--u", "0.1"], 0.1),
-    ("QbitMode_C++QED", ["--picture", "IP", "--deltaA", "-1", "--gamma", "0.5", "--deltaC", "2", "--kappa", "1",
-                         "--eta", "1.5", "--cutoff", "100", "--g", "2"], 0.2),
-]
-
-
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("case", range(len(FACTORED_CASES)))
-def test_factored_operator_matches_ell_tables(gpu, case, precision):
-    """The CTA kernel's per-axis operator (a row's coefficient a product of one factor per
-    axis, phases per factor entry) against the row tables with per-row phases
-    (ip_phase_table = -1, the reference's arithmetic): the same trajectories to rounding."""
-    script, args, Dt = FACTORED_CASES[case]
-    model = gpu.Model(script, args)
-    assert model.dim > 128
-    sysd = gpu.System(model.desc)
-    n = 12
-    out = []
-    for table in (0, -1):
-        pars = model.run_pars().mcwf
-        pars.precision = A.FP64 if precision == "fp64" else A.FP32
-        pars.ip_phase_table = table
-        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
-        assert ens.plan()[0]["kind"] in (1, 2)
-        sums = ens.run(Dt, 2)
-        out.append((sums, np.stack([ens.state(i, model.dim) for i in range(n)]), [ens.jumps(i) for i in range(n)]))
-    (s0, x0, j0), (s1, x1, j1) = out
-    tol, rt = (1e-8, 1e-8) if precision == "fp64" else (2e-4, 1e-4)
-    agree = 0
-    for i in range(n):
-        (ta, la), (tb, lb) = j0[i], j1[i]
-        if len(ta) == len(tb) and np.allclose(ta, tb, rtol=rt) and np.array_equal(la, lb):
-            agree += 1
-            assert np.linalg.norm(x0[i] - x1[i]) < tol * max(1.0, np.linalg.norm(x1[i]))
-    assert agree >= n - 1
-
-
 def test_block_kernel_cta_shapes_agree(gpu):
     """The CTA-per-trajectory kernel with 64, 160, 256 and 512 threads (one to eight rows per
     thread at D = 450) follows the same trajectories up to the summation order."""
