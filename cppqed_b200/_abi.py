@@ -95,6 +95,7 @@ class cqg_mcwf_pars(C.Structure):
         ("cta_threads", C.c_int32),
         ("cta_shared_vectors", C.c_int32),
         ("ip_phase_table", C.c_int32),
+        ("yield_steps", C.c_int32),
     ]
 
 

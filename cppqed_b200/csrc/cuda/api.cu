@@ -58,6 +58,10 @@ class HostStaging {
 // single device allocation carved into aligned sub-buffers
 // autotuner shape bit: the warp kernel's instance compiled for more resident CTAs
 constexpr int kHighOccupancyFlag = 1 << 17;
+// MCWF steps after which a warp hands its trajectory back to the work queue (cqg_mcwf_pars::
+// yield_steps = 0), and push slots per trajectory and launch
+constexpr int kDefaultYieldSteps = 32;
+constexpr int64_t kYieldSlotsPerTrajectory = 64;
 
 struct Arena {
   std::vector<std::pair<size_t, size_t>> parts;  // offset, size
@@ -99,6 +103,14 @@ struct cqg_ensemble {
   int jumpCap = 64;
   void* dJumpRing = nullptr;  // jump rings of a grown capacity (cqg_ensemble_set_jump_capacity)
   size_t jumpRingBytes = 0;
+  // warp-kernel yielding (RunArgs::yieldSteps): per group 4 header ints (push tail, finished
+  // trajectories, error, pad) and the push marks, then every trajectory's ResumeInfo (these
+  // zeroed before each launch), then per group the pushed trajectory indices
+  void* dYield = nullptr;
+  size_t yieldBytes = 0, yieldZeroBytes = 0;
+  std::vector<size_t> yieldHead, yieldSeq, yieldEntry;  // byte offsets per group
+  std::vector<int> yieldCap;
+  size_t yieldResume = 0;
   ~cqg_ensemble() {
     // nothing of this ensemble may still run on the blocks that go back to the cache
     int cur = 0;
@@ -116,6 +128,7 @@ struct cqg_ensemble {
     cqg::engine::deviceRelease(device, dSums, sumsCap * sizeof(double));
     cqg::engine::deviceRelease(device, dmem, dmemBytes);
     cqg::engine::deviceRelease(device, dJumpRing, jumpRingBytes);
+    cqg::engine::deviceRelease(device, dYield, yieldBytes);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evRun0) cudaEventDestroy(evRun0);
@@ -824,6 +837,7 @@ void launchGroup(bool fp64, size_t elemBytes, const dev::TrajDev& td, KernelGrou
        "occupancy");
     int grid = int(std::min<int64_t>(int64_t(std::max(perSM, 1)) * nSM, (g.count + warps - 1) / warps));
     grid = std::max(grid, 1);
+    if (g.count <= int64_t(grid) * warps) ra.yieldSteps = 0;  // one wave: nothing to balance
     void* args[] = {&tdArg, &ra};
     ck(cudaLaunchKernel(reinterpret_cast<const void*>(fn), dim3(grid), dim3(g.threads), args, smem, st),
        "kernel launch");
@@ -917,6 +931,38 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
 
   int nSM = 0;
   ck(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, e->device), "attribute");
+  // warp groups hand their trajectories back to the queue every yield_steps MCWF steps
+  const int yieldSteps = ra.mode == dev::RUN_STEPS || e->pars.yield_steps < 0 ? 0
+                         : e->pars.yield_steps > 0                           ? e->pars.yield_steps
+                                                                              : kDefaultYieldSteps;
+  if (yieldSteps > 0 && !e->dYield) {
+    size_t off = 0;
+    const size_t nG = e->groups.size();
+    e->yieldHead.assign(nG, 0);
+    e->yieldSeq.assign(nG, 0);
+    e->yieldEntry.assign(nG, 0);
+    e->yieldCap.assign(nG, 0);
+    for (size_t gi = 0; gi < nG; ++gi) {
+      e->yieldCap[gi] = int(std::min<int64_t>(e->groups[gi].count * kYieldSlotsPerTrajectory, int64_t(1) << 28));
+      e->yieldHead[gi] = off;
+      off += 16;
+    }
+    for (size_t gi = 0; gi < nG; ++gi) {
+      e->yieldSeq[gi] = off;
+      off += size_t(e->yieldCap[gi]) * 4;
+    }
+    off = (off + 15) / 16 * 16;
+    e->yieldResume = off;
+    off += size_t(e->nTraj) * sizeof(dev::ResumeInfo);
+    e->yieldZeroBytes = off;
+    for (size_t gi = 0; gi < nG; ++gi) {
+      e->yieldEntry[gi] = off;
+      off += size_t(e->yieldCap[gi]) * 4;
+    }
+    e->dYield = deviceAlloc(off, "cudaMalloc(yield queues)");
+    e->yieldBytes = off;
+  }
+  if (yieldSteps > 0) ck(cudaMemsetAsync(e->dYield, 0, e->yieldZeroBytes, e->stream), "cudaMemsetAsync");
   ck(cudaEventRecord(e->ev0, e->stream), "cudaEventRecord");
   const bool fork = e->groups.size() > 1;
   if (fork) ck(cudaEventRecord(e->evFork, e->stream), "cudaEventRecord");
@@ -927,6 +973,18 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
     ra.order = e->dOrder + g.first;
     ra.nTasks = int(g.count);
     ra.queue = e->dQueue + gi;
+    ra.yieldSteps = g.kind == 0 ? yieldSteps : 0;
+    if (ra.yieldSteps > 0) {
+      char* y = static_cast<char*>(e->dYield);
+      int* head = reinterpret_cast<int*>(y + e->yieldHead[gi]);
+      ra.yieldTail = head;
+      ra.doneCount = head + 1;
+      ra.queueError = reinterpret_cast<unsigned*>(head + 2);
+      ra.yieldSeq = reinterpret_cast<int*>(y + e->yieldSeq[gi]);
+      ra.yieldEntry = reinterpret_cast<int*>(y + e->yieldEntry[gi]);
+      ra.yieldCap = e->yieldCap[gi];
+      ra.resume = reinterpret_cast<dev::ResumeInfo*>(y + e->yieldResume);
+    }
     launchGroup(e->pars.precision == CQG_FP64, e->elemBytes, e->td, g, ra, nSM, st);
     if (fork) {
       ck(cudaEventRecord(g.done, st), "cudaEventRecord");
@@ -943,6 +1001,11 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   ck(cudaGetLastError(), "status launch");
   unsigned bits = 0;
   ck(cudaMemcpyAsync(&bits, e->dStatusOr, sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream), "cudaMemcpyAsync");
+  std::vector<int> yieldHeads(yieldSteps > 0 ? 4 * e->groups.size() : 0);
+  for (size_t gi = 0; gi < e->groups.size() && yieldSteps > 0; ++gi)
+    ck(cudaMemcpyAsync(&yieldHeads[4 * gi], static_cast<char*>(e->dYield) + e->yieldHead[gi], 16,
+                       cudaMemcpyDeviceToHost, e->stream),
+       "cudaMemcpyAsync");
   std::vector<double> sums;
   if (avrHost && nAvr > 0 && nOut > 0) {
     ck(cudaMemcpyAsync(avrHost, e->dSums, size_t(nOut) * nAvr * sizeof(double), cudaMemcpyDeviceToHost, e->stream),
@@ -954,6 +1017,9 @@ int launchRun(cqg_ensemble* e, dev::RunArgs ra, int nOut, double* avrHost) {
   ck(cudaEventElapsedTime(&e->lastRunMs, e->evRun0, e->evRun1), "cudaEventElapsedTime");
   if (bits & 3u) return fail(CQG_E_NONFINITE, "a trajectory produced a non-finite norm or rate");
   if (bits & 12u) return fail(CQG_E_STALLED, "a trajectory exhausted its step-size or attempt budget");
+  for (size_t gi = 0; 4 * gi < yieldHeads.size(); ++gi)
+    if (yieldHeads[4 * gi + 2])
+      return fail(CQG_E_STALLED, "a yielded trajectory was not resumed within the time limit");
   return CQG_OK;
 }
 

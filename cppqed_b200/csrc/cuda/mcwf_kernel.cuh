@@ -302,6 +302,29 @@ struct RunArgs {
   const int* order;  // the launch's trajectories (a segment of the ensemble's order)
   int nTasks;        // how many
   int phaseCache;    // warp kernel: shared memory holds a per-warp interaction-picture phase table
+  // Warp kernel, RUN_INTERVALS / RUN_TO: a warp yields its trajectory after yieldSteps MCWF
+  // steps (0: never) and takes the next task, so that the end of a launch is one chunk of
+  // steps long rather than one whole trajectory.  A yielding warp saves the trajectory with
+  // its place in the run (ResumeInfo), reserves the next push slot (yieldTail) and publishes
+  // the trajectory there (yieldEntry, then yieldSeq = slot + 1); tasks past nTasks are these
+  // pushes in order.  When the slots run out (yieldCap) trajectories run on without yielding.
+  int yieldSteps;
+  int yieldCap;
+  int* yieldTail;
+  int* yieldEntry;
+  int* yieldSeq;
+  int* doneCount;     // trajectories of the launch that finished
+  unsigned* queueError;  // set when a wait for a published push ran past the time limit
+  struct ResumeInfo* resume;  // [trajectory] place of a yielded trajectory in the run
+};
+
+// Where a yielded trajectory resumes: output interval k, the end time and step count of the
+// interval it is in (mid != 0).  Zeroed before every launch.
+struct ResumeInfo {
+  double endTime;
+  long long guard;
+  int k;
+  int mid;
 };
 
 // Cash-Karp tableau (published coefficients)
@@ -817,7 +840,7 @@ struct Worker {
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(jx[e].x) * inv, double(jx[e].y) * inv);
       if (lane == 0 && td.jumpCap > 0) {
-        const unsigned long long total = td.jumpN[ti] + nJumps;
+        const unsigned long long total = __ldcg(&td.jumpN[ti]) + nJumps;
         const unsigned long long slot = total % (unsigned long long)td.jumpCap;
         td.jumpT[ti * td.jumpCap + slot] = t;
         td.jumpL[ti * td.jumpCap + slot] = lindbladNo;
@@ -888,35 +911,63 @@ struct Worker {
     __syncwarp();
   }
 
-  __device__ __forceinline__ void run(const TrajDev& td, int trajIndex) {
+  // One task: advances the trajectory through the run (its output intervals, or to its end
+  // time), or, with ra.yieldSteps > 0, until it has taken that many MCWF steps and a push slot
+  // was reserved for it: then it saves its place (ResumeInfo), writes *pushSlot and returns
+  // false.  A trajectory may resume on another SM, so its state is read past L1 (__ldcg).
+  __device__ __forceinline__ bool run(const TrajDev& td, int trajIndex, int* pushSlot) {
     ti = (unsigned long long)trajIndex;
     C2* psi = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
     loadOperator();
 #pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = valid(e) ? psi[row(e)] : mk<C2>(0, 0);
-    t = td.t[ti];
-    t0 = td.t0[ti];
-    dtTry = td.dtTry[ti];
-    dtDid = td.dtDid[ti];
-    if (lane < 4) ws->pcg[lane] = td.rng[4 * ti + lane];
+    for (int e = 0; e < E; ++e) x[e] = valid(e) ? __ldcg(&psi[row(e)]) : mk<C2>(0, 0);
+    t = __ldcg(&td.t[ti]);
+    t0 = __ldcg(&td.t0[ti]);
+    dtTry = __ldcg(&td.dtTry[ti]);
+    dtDid = __ldcg(&td.dtDid[ti]);
+    if (lane < 4) ws->pcg[lane] = __ldcg(&td.rng[4 * ti + lane]);
     __syncwarp();
     nSteps = nAttempts = nFailed = nRhs = nOvershot = nBacks = nJumps = 0;
-    maxOvershoot = td.maxima[3 * ti];
-    maxTolOvershoot = td.maxima[3 * ti + 1];
-    maxNormDev = td.maxima[3 * ti + 2];
-    status = td.status[ti];
+    maxOvershoot = __ldcg(&td.maxima[3 * ti]);
+    maxTolOvershoot = __ldcg(&td.maxima[3 * ti + 1]);
+    maxNormDev = __ldcg(&td.maxima[3 * ti + 2]);
+    status = __ldcg(&td.status[ti]);
+    ResumeInfo rs{0., 0, 0, 0};
+    if (ra.resume) {
+      rs.endTime = __ldcg(&ra.resume[ti].endTime);
+      rs.guard = __ldcg(&ra.resume[ti].guard);
+      rs.k = __ldcg(&ra.resume[ti].k);
+      rs.mid = __ldcg(&ra.resume[ti].mid);
+    }
 
     const int nOut = ra.mode == RUN_TO ? 1 : ra.nIntervals;
     const unsigned long long tStart = globalTimerNs();
-    for (int k = 0; k < nOut && status == 0u; ++k) {
-      long long guard = 0;
+    bool yielded = false, mayYield = ra.yieldSteps > 0 && ra.mode != RUN_STEPS;
+    int chunkSteps = 0;
+    int k = rs.k;
+    for (; k < nOut && status == 0u; ++k) {
+      long long guard = rs.mid ? rs.guard : 0;
       if (ra.mode == RUN_STEPS) {
         for (int s = 0; s < ra.nSteps && t < ra.T; ++s)
           if (!step(ra.T - t, td)) break;
       } else {
-        const double endTime = ra.mode == RUN_TO ? (ra.tEndPer ? ra.tEndPer[ti] : ra.tEnd) : t + ra.Dt;
+        const double endTime =
+            rs.mid ? rs.endTime : ra.mode == RUN_TO ? (ra.tEndPer ? ra.tEndPer[ti] : ra.tEnd) : t + ra.Dt;
+        rs.mid = 0;
         double dt;
         while ((dt = endTime - t) != 0.) {
+          if (mayYield && chunkSteps >= ra.yieldSteps) {
+            int slot = 0;
+            if (lane == 0) slot = atomicAdd(ra.yieldTail, 1);
+            slot = __shfl_sync(FULL, slot, 0);
+            if (slot < ra.yieldCap) {
+              rs = ResumeInfo{endTime, guard, k, 1};
+              *pushSlot = slot;
+              yielded = true;
+              break;
+            }
+            mayYield = false;  // no push slot left: run on
+          }
           // bounded: a negative remainder, a step budget, or the wall-clock watchdog
           // end the trajectory with an error status instead of spinning
           if (dt < 0. || ++guard > ra.maxStepsPerInterval ||
@@ -925,8 +976,10 @@ struct Worker {
             break;
           }
           if (!step(dt, td)) break;
+          ++chunkSteps;
         }
       }
+      if (yielded) break;
       if (ra.avrOut) {
         double* slot = ra.avrOut + ((size_t)k * td.nTraj + ti) * ra.nAvrStride;
         averages(slot);
@@ -945,20 +998,23 @@ struct Worker {
       td.dtTry[ti] = dtTry;
       td.dtDid[ti] = dtDid;
       unsigned long long* cw = td.cnt + 8 * ti;
-      cw[0] += nSteps;
-      cw[1] += nAttempts;
-      cw[2] += nFailed;
-      cw[3] += nRhs;
-      cw[4] += nOvershot;
-      cw[5] += nBacks;
-      cw[6] += nJumps;
+      cw[0] = __ldcg(&cw[0]) + nSteps;
+      cw[1] = __ldcg(&cw[1]) + nAttempts;
+      cw[2] = __ldcg(&cw[2]) + nFailed;
+      cw[3] = __ldcg(&cw[3]) + nRhs;
+      cw[4] = __ldcg(&cw[4]) + nOvershot;
+      cw[5] = __ldcg(&cw[5]) + nBacks;
+      cw[6] = __ldcg(&cw[6]) + nJumps;
       cw[7] = status;
       td.maxima[3 * ti] = maxOvershoot;
       td.maxima[3 * ti + 1] = maxTolOvershoot;
       td.maxima[3 * ti + 2] = maxNormDev;
       td.status[ti] = status;
-      td.jumpN[ti] += nJumps;
+      td.jumpN[ti] = __ldcg(&td.jumpN[ti]) + nJumps;
+      if (ra.resume) ra.resume[ti] = yielded ? rs : ResumeInfo{0., 0, nOut, 0};
     }
+    __syncwarp();
+    return !yielded;
     __syncwarp();
   }
 };
@@ -1004,10 +1060,52 @@ __global__ void __launch_bounds__(128, MINB) mcwfWarpKernel(TrajDev td, RunArgs 
     int task = 0;
     if (lane == 0) task = atomicAdd(ra.queue, 1);
     task = __shfl_sync(FULL, task, 0);
-    if (task >= ra.nTasks) return;
-    const int ti = ra.order[task];
+    int ti;
+    if (task < ra.nTasks) {
+      ti = ra.order[task];
+    } else {
+      // Tasks past nTasks are the yielded trajectories in push order.  Wait until push p is
+      // published, or every trajectory of the launch is done (no push will come), or the
+      // wall-clock limit passes (an error the host reports).
+      const int p = task - ra.nTasks;
+      if (ra.yieldSteps <= 0 || p >= ra.yieldCap) return;
+      int got = -1;
+      if (lane == 0) {
+        const unsigned long long tw = globalTimerNs();
+        volatile int* seq = ra.yieldSeq;
+        volatile int* done = ra.doneCount;
+        while (true) {
+          if (seq[p] == p + 1) {
+            __threadfence();
+            got = reinterpret_cast<volatile int*>(ra.yieldEntry)[p];
+            break;
+          }
+          if (*done >= ra.nTasks) break;
+          if (globalTimerNs() - tw > ra.timeLimitNs) {
+            atomicOr(ra.queueError, 1u);
+            break;
+          }
+          __nanosleep(256);
+        }
+      }
+      got = __shfl_sync(FULL, got, 0);
+      if (got < 0) return;
+      ti = got;
+    }
     Worker<R, E, SMAX, IP> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws, phs);
-    w.run(td, ti);
+    int slot = -1;
+    const bool finished = w.run(td, ti, &slot);
+    __threadfence();  // the trajectory's state is visible before it is counted or published
+    __syncwarp();
+    if (lane == 0) {
+      if (finished) {
+        atomicAdd(ra.doneCount, 1);
+      } else {
+        ra.yieldEntry[slot] = ti;
+        __threadfence();
+        atomicExch(&ra.yieldSeq[slot], slot + 1);
+      }
+    }
   }
 }
 

@@ -30,7 +30,7 @@ extern "C" {
 #endif
 
 #define CQG_MAX_RANK 8
-#define CQG_ABI_VERSION 4
+#define CQG_ABI_VERSION 5
 
 /* ---- status codes ------------------------------------------------------ */
 #define CQG_OK 0
@@ -161,6 +161,12 @@ typedef struct cqg_mcwf_pars {
                                   stage powers of exp(dt f / 40); at most 1024 on the CTA
                                   kernel: per stage, bit-identical to -1), -1 forms them per
                                   row, slot and stage as the reference does */
+  int32_t yield_steps;         /* warp-per-trajectory groups of more trajectories than the GPU
+                                  holds at once: a warp hands its trajectory back to the work
+                                  queue after this many MCWF steps and takes the next, so the
+                                  end of a launch waits for one such chunk, not for whole
+                                  trajectories; the results are bit-identical.  0: the default
+                                  (32), -1: never */
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);

@@ -31,7 +31,7 @@ def test_ctypes_mirror_covers_the_headers():
 
 def test_abi_version_and_error_channel(engine):
     lib = engine.lib()
-    assert lib.cqg_abi_version() == 4
+    assert lib.cqg_abi_version() == 5
     h = ctypes.c_void_p()
     rc = lib.cqg_model_create(b"NoSuchScript", 0, None, ctypes.byref(h))
     assert rc == A.CQG_E_INVALID

@@ -469,6 +469,42 @@ def test_warp_kernel_occupancy_instances_agree(gpu):
         assert np.array_equal(st, out[0][0]) and np.array_equal(t, out[0][1]) and np.array_equal(c, out[0][2])
 
 
+@pytest.mark.parametrize("script,args", [
+    ("QbitMode_C++QED", C2_ARGS),
+    ("QbitMode_C++QED", ["--picture", "IP", "--deltaA", "-1", "--gamma", "0.5", "--deltaC", "2", "--kappa", "1",
+                         "--eta", "1.5", "--cutoff", "40", "--g", "2"]),
+    ("PumpedLossyMode_C++QED", C1_ARGS),
+])
+def test_yielding_trajectories_are_bit_identical(gpu, script, args):
+    """More trajectories than the GPU holds at once: warps hand their trajectories back to the
+    work queue every yield_steps MCWF steps (1: every step, 0: the default, 32) and resume them
+    anywhere, which leaves every state, time, counter, jump record and output row bit-identical
+    to never yielding (-1); also across two run calls and over several output intervals."""
+    model = gpu.Model(script, args)
+    sysd = gpu.System(model.desc)
+    n = 6000
+    out = []
+    for ys in (-1, 0, 1):
+        pars = model.run_pars().mcwf
+        pars.autotune = 0
+        pars.cta_threads = 128
+        pars.yield_steps = ys
+        ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+        rows = np.concatenate([ens.run(0.3, 3), ens.run(0.2, 1)])
+        pick = range(0, n, 131)
+        out.append((rows, np.stack([ens.state(i, model.dim) for i in pick]), ens.times(), ens.counters(),
+                    [ens.jumps(i) for i in pick]))
+    ref = out[0]
+    for got in out[1:]:
+        assert np.array_equal(got[0], ref[0])
+        assert np.array_equal(got[1], ref[1])
+        for a, b in zip(got[2], ref[2]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(got[3], ref[3])
+        for (ta, la), (tb, lb) in zip(got[4], ref[4]):
+            assert np.array_equal(ta, tb) and np.array_equal(la, lb)
+
+
 def test_block_kernel_cta_shapes_agree(gpu):
     """The CTA-per-trajectory kernel with 64, 160, 256 and 512 threads (one to eight rows per
     thread at D = 450) follows the same trajectories up to the summation order."""
