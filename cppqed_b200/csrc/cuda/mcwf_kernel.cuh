@@ -1011,7 +1011,7 @@ struct Worker {
       td.maxima[3 * ti + 2] = maxNormDev;
       td.status[ti] = status;
       td.jumpN[ti] = __ldcg(&td.jumpN[ti]) + nJumps;
-      if (ra.resume) ra.resume[ti] = yielded ? rs : ResumeInfo{0., 0, nOut, 0};
+      if (yielded) ra.resume[ti] = rs;
     }
     __syncwarp();
     return !yielded;
@@ -1095,15 +1095,17 @@ __global__ void __launch_bounds__(128, MINB) mcwfWarpKernel(TrajDev td, RunArgs 
     Worker<R, E, SMAX, IP> w(td.systems + td.sysIdx[ti], ra, lane, base, base + DMAX, base + 2 * DMAX, ws, phs);
     int slot = -1;
     const bool finished = w.run(td, ti, &slot);
-    __threadfence();  // the trajectory's state is visible before it is counted or published
-    __syncwarp();
-    if (lane == 0) {
-      if (finished) {
-        atomicAdd(ra.doneCount, 1);
-      } else {
-        ra.yieldEntry[slot] = ti;
-        __threadfence();
-        atomicExch(&ra.yieldSeq[slot], slot + 1);
+    if (ra.yieldSteps > 0) {  // the queue's counters and marks exist only when yielding is on
+      __threadfence();        // the trajectory's state is visible before it is counted or published
+      __syncwarp();
+      if (lane == 0) {
+        if (finished) {
+          atomicAdd(ra.doneCount, 1);
+        } else {
+          ra.yieldEntry[slot] = ti;
+          __threadfence();
+          atomicExch(&ra.yieldSeq[slot], slot + 1);
+        }
       }
     }
   }
