@@ -134,6 +134,8 @@ def parse():
     ap.add_argument("--cta-shared-vectors", type=int, default=0,
                     help="with --cta-threads: 1 selects the shared-memory stage vectors (CTA kernel) or the "
                          "high-occupancy instance (warp kernel)")
+    ap.add_argument("--yield-steps", type=int, default=0,
+                    help="MCWF steps after which a warp hands its trajectory back to the queue (0: default, -1: never)")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave out the batched-vs-plain, accuracy and serving checks of the default line")
     ap.add_argument("--apply-states", type=int, default=0,
@@ -304,6 +306,7 @@ def run_ours(args, rank, world, dev):
     pars.rng = A.RNG_PCG64 if args.rng == "pcg64" else A.RNG_PHILOX
     pars.precision = A.FP64 if args.precision == "fp64" else A.FP32
     pars.prng_stream = sharding.first_stream(1, n_traj, rank)
+    pars.yield_steps = args.yield_steps
     if args.cta_threads:
         pars.autotune = 0
         pars.cta_threads = args.cta_threads

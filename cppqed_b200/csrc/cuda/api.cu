@@ -60,7 +60,7 @@ class HostStaging {
 constexpr int kHighOccupancyFlag = 1 << 17;
 // MCWF steps after which a warp hands its trajectory back to the work queue (cqg_mcwf_pars::
 // yield_steps = 0), and push slots per trajectory and launch
-constexpr int kDefaultYieldSteps = 32;
+constexpr int kDefaultYieldSteps = 64;
 constexpr int64_t kYieldSlotsPerTrajectory = 64;
 
 struct Arena {

@@ -166,7 +166,7 @@ typedef struct cqg_mcwf_pars {
                                   queue after this many MCWF steps and takes the next, so the
                                   end of a launch waits for one such chunk, not for whole
                                   trajectories; the results are bit-identical.  0: the default
-                                  (32), -1: never */
+                                  (64), -1: never */
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);
