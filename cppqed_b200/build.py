@@ -21,7 +21,7 @@ HOST_SOURCES = ["host/tridiagonal.cpp", "host/elements.cpp", "host/model.cpp", "
                 "host/scripts.cpp", "host/errors.cpp", "host/api_model.cpp", "host/lowering.cpp"]
 CUDA_SOURCES = ["cuda/api.cu", "cuda/noalloc.cu", "cuda/kernels_block.cu", "cuda/apply.cu", "cuda/server.cu", "cuda/master.cu"]
 # the kernel instantiations: one object per (precision, rows per lane)
-KERNEL_INSTANCES = [(r, e) for r in ("double", "float") for e in (1, 2, 3, 4)]
+KERNEL_INSTANCES = [(r, e, ip) for r in ("double", "float") for e in (1, 2, 3, 4) for ip in (0, 1)]
 # what each kind of object is rebuilt for (besides its own source and include/*.h)
 HOST_HEADERS = ["host/lowering.hpp", "host/errors.hpp", "host/model.hpp", "host/elements.hpp", "host/tridiagonal.hpp",
                 "host/pars.hpp"]
@@ -106,9 +106,10 @@ def build(verbose=False, ptxas_info=False, extra_flags=(), lib=None):
         o = os.path.join(OBJDIR, os.path.basename(src) + ".o")
         jobs.append((s, o, [], deps(CUDA_HEADERS)))
     inst = os.path.join(CSRC, "cuda", "kernels_inst.cu")
-    for r, e in KERNEL_INSTANCES:
-        jobs.append((inst, os.path.join(OBJDIR, "kernels_%s_e%d.o" % (r, e)),
-                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e], deps(KERNEL_HEADERS, with_public=False)))
+    for r, e, ip in KERNEL_INSTANCES:
+        jobs.append((inst, os.path.join(OBJDIR, "kernels_%s_e%d_ip%d.o" % (r, e, ip)),
+                     ["-DCQG_REAL=" + r, "-DCQG_E=%d" % e, "-DCQG_IP=%d" % ip],
+                     deps(KERNEL_HEADERS, with_public=False)))
     procs = []
     for s, o, defs, hdrs in jobs:
         objs.append(o)

@@ -347,6 +347,30 @@ void buildSystemDevice(cqg_system& s) {
       fIdx[i] = static_cast<unsigned short>(it->second);
     }
   }
+  // The CTA kernel's packed slot records (see SysDev::ctaWord)
+  const bool ctaRecords = D < 32768;
+  std::vector<int> ctaWord;
+  std::vector<int4> ctaRecF;
+  if (ctaRecords && S > 0) {
+    ctaWord.resize(size_t(S) * D);
+    ctaRecF.resize(size_t(S) * D);
+    for (int k = 0; k < S; ++k)
+      for (int64_t r = 0; r < D; ++r) {
+        const size_t o = size_t(k) * D + r;
+        const int off = H.col[o] - int(r);
+        const unsigned fi = fIdx.empty() ? unsigned(dev::kNoPhase) : unsigned(fIdx[o]);
+        const unsigned word = (fi << 16) | (unsigned(off) & 0xffffu);
+        ctaWord[o] = int(word);
+        const float vx = float(H.val[o].real()), vy = float(H.val[o].imag());
+        int4 rec;
+        std::memcpy(&rec.x, &vx, 4);
+        std::memcpy(&rec.y, &vy, 4);
+        rec.z = int(word);
+        rec.w = 0;
+        ctaRecF[o] = rec;
+      }
+  }
+  const size_t oCtaWord = A.add(ctaWord.size() * 4 + 16), oCtaRecF = A.add(ctaRecF.size() * 16 + 16);
   // The warp kernel's padded copies of the hot tables (see SysDev::wcol): rows to
   // Dp = 32 ceil(D / 32), slots to kWarpSlots, zero coefficients on the row itself.
   const bool warpTables = D <= kWarpKernelMaxD && S <= dev::kWarpSlots;
@@ -422,6 +446,8 @@ void buildSystemDevice(cqg_system& s) {
   upload(b, oDiagF, toF2(H.diag));
   upload(b, oValF, toF2(H.val));
   upload(b, oJvalF, toF2(jval));
+  upload(b, oCtaWord, ctaWord);
+  upload(b, oCtaRecF, ctaRecF);
   upload(b, oWcol, wcol);
   upload(b, oWdiagD, toD2(wdiag));
   upload(b, oWvalD, toD2(wval));
@@ -470,6 +496,11 @@ void buildSystemDevice(cqg_system& s) {
   sd.diagF = reinterpret_cast<const float2*>(b + oDiagF);
   sd.valF = reinterpret_cast<const float2*>(b + oValF);
   sd.jvalF = reinterpret_cast<const float2*>(b + oJvalF);
+  sd.diagZero = 1;
+  for (const auto& v : H.diag)
+    if (v != dcomp(0, 0)) sd.diagZero = 0;
+  sd.ctaWord = ctaWord.empty() ? nullptr : reinterpret_cast<const int*>(b + oCtaWord);
+  sd.ctaRecF = ctaRecF.empty() ? nullptr : reinterpret_cast<const int4*>(b + oCtaRecF);
   sd.Dp = warpTables ? int(Dp) : 0;
   sd.wcol = warpTables ? reinterpret_cast<const int*>(b + oWcol) : nullptr;
   sd.wdiagD = warpTables ? reinterpret_cast<const double2*>(b + oWdiagD) : nullptr;
@@ -490,14 +521,22 @@ using KernelFn = void (*)(dev::TrajDev, dev::RunArgs);
 
 namespace cqg {
 namespace dev {
-KernelFn pick_double_e1(int smax, bool ip, bool highOccupancy);
-KernelFn pick_double_e2(int smax, bool ip, bool highOccupancy);
-KernelFn pick_double_e3(int smax, bool ip, bool highOccupancy);
-KernelFn pick_double_e4(int smax, bool ip, bool highOccupancy);
-KernelFn pick_float_e1(int smax, bool ip, bool highOccupancy);
-KernelFn pick_float_e3(int smax, bool ip, bool highOccupancy);
-KernelFn pick_float_e2(int smax, bool ip, bool highOccupancy);
-KernelFn pick_float_e4(int smax, bool ip, bool highOccupancy);
+KernelFn pick_double_e1_ip0(int smax, bool highOccupancy);
+KernelFn pick_double_e1_ip1(int smax, bool highOccupancy);
+KernelFn pick_double_e2_ip0(int smax, bool highOccupancy);
+KernelFn pick_double_e2_ip1(int smax, bool highOccupancy);
+KernelFn pick_double_e3_ip0(int smax, bool highOccupancy);
+KernelFn pick_double_e3_ip1(int smax, bool highOccupancy);
+KernelFn pick_double_e4_ip0(int smax, bool highOccupancy);
+KernelFn pick_double_e4_ip1(int smax, bool highOccupancy);
+KernelFn pick_float_e1_ip0(int smax, bool highOccupancy);
+KernelFn pick_float_e1_ip1(int smax, bool highOccupancy);
+KernelFn pick_float_e2_ip0(int smax, bool highOccupancy);
+KernelFn pick_float_e2_ip1(int smax, bool highOccupancy);
+KernelFn pick_float_e3_ip0(int smax, bool highOccupancy);
+KernelFn pick_float_e3_ip1(int smax, bool highOccupancy);
+KernelFn pick_float_e4_ip0(int smax, bool highOccupancy);
+KernelFn pick_float_e4_ip1(int smax, bool highOccupancy);
 }  // namespace dev
 }  // namespace cqg
 
@@ -520,15 +559,13 @@ int tunedThreads(const cqg_ensemble& e, size_t gi, const cqg_system* const* syst
 bool sharedVectorsFit(const KernelGroup& g, size_t elemBytes, int device);
 
 KernelFn pickKernel(bool fp64, int E, int SMAX, bool ip, bool hi) {
-  if (fp64)
-    return E == 1 ? dev::pick_double_e1(SMAX, ip, hi)
-         : E == 2 ? dev::pick_double_e2(SMAX, ip, hi)
-         : E == 3 ? dev::pick_double_e3(SMAX, ip, hi)
-                  : dev::pick_double_e4(SMAX, ip, hi);
-  return E == 1 ? dev::pick_float_e1(SMAX, ip, hi)
-       : E == 2 ? dev::pick_float_e2(SMAX, ip, hi)
-       : E == 3 ? dev::pick_float_e3(SMAX, ip, hi)
-                : dev::pick_float_e4(SMAX, ip, hi);
+  using P = KernelFn (*)(int, bool);
+  static const P table[2][4][2] = {
+      {{dev::pick_double_e1_ip0, dev::pick_double_e1_ip1}, {dev::pick_double_e2_ip0, dev::pick_double_e2_ip1},
+       {dev::pick_double_e3_ip0, dev::pick_double_e3_ip1}, {dev::pick_double_e4_ip0, dev::pick_double_e4_ip1}},
+      {{dev::pick_float_e1_ip0, dev::pick_float_e1_ip1}, {dev::pick_float_e2_ip0, dev::pick_float_e2_ip1},
+       {dev::pick_float_e3_ip0, dev::pick_float_e3_ip1}, {dev::pick_float_e4_ip0, dev::pick_float_e4_ip1}}};
+  return table[fp64 ? 0 : 1][std::min(std::max(E, 1), 4) - 1][ip ? 1 : 0](SMAX, hi);
 }
 
 __global__ void reduceAveragesKernel(const double* __restrict__ avr, int nTraj, int nAvrStride, int nAvr,

@@ -1,7 +1,7 @@
-// Explicit instantiation of the fused MCWF warp kernel for one (precision, rows per
-// lane) pair; the build compiles this file once per pair (-DCQG_REAL, -DCQG_E) so the
-// instances compile in parallel.  Exposes pick_<real>_e<E>(SMAX, interaction picture, high
-// occupancy).
+// Explicit instantiation of the fused MCWF warp kernel for one (precision, rows per lane,
+// picture) triple; the build compiles this file once per triple (-DCQG_REAL, -DCQG_E,
+// -DCQG_IP) so the instances compile in parallel.  Exposes
+// pick_<real>_e<E>_ip<IP>(SMAX, high occupancy).
 #include "mcwf_kernel.cuh"
 
 #ifndef CQG_REAL
@@ -10,9 +10,12 @@
 #ifndef CQG_E
 #error "CQG_E must be defined"
 #endif
+#ifndef CQG_IP
+#error "CQG_IP must be defined"
+#endif
 
-#define CQG_CAT2(a, b, c) a##b##_e##c
-#define CQG_CAT(a, b, c) CQG_CAT2(a, b, c)
+#define CQG_CAT2(a, b, c, d) a##b##_e##c##_ip##d
+#define CQG_CAT(a, b, c, d) CQG_CAT2(a, b, c, d)
 
 namespace cqg {
 namespace dev {
@@ -30,16 +33,12 @@ KernelFn pickOccupancy(bool highOccupancy) {
   return &mcwfWarpKernel<CQG_REAL, CQG_E, SMAX, IP, WarpMinBlocks<CQG_E, IP>::value>;
 }
 
-template <bool IP>
-KernelFn pickSlots(int smax, bool highOccupancy) {
+KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E, CQG_IP)(int smax, bool highOccupancy) {
+  constexpr bool IP = CQG_IP != 0;
   if (smax <= 2) return pickOccupancy<2, IP>(highOccupancy);
   if (smax <= 3) return pickOccupancy<3, IP>(highOccupancy);
   if (smax <= 4) return pickOccupancy<4, IP>(highOccupancy);
   return pickOccupancy<8, IP>(highOccupancy);
-}
-
-KernelFn CQG_CAT(pick_, CQG_REAL, CQG_E)(int smax, bool ip, bool highOccupancy) {
-  return ip ? pickSlots<true>(smax, highOccupancy) : pickSlots<false>(smax, highOccupancy);
 }
 
 }  // namespace dev

@@ -80,6 +80,9 @@ struct BlockWorker {
   const double2* fDist;
   int nFD;
   double2* phTab;  // IP: shared-memory phases of the distinct frequencies, or null
+  const int* word;    // packed slot words (SysDev::ctaWord) or null
+  const int4* recF;   // FP32 packed records (SysDev::ctaRecF) or null
+  bool diagZero;      // the fused main diagonal is zero: not read
   C2* x;       // the trajectory's state (device memory)
   C2* vec;     // this CTA's scratch vectors
   long long stride;
@@ -116,9 +119,24 @@ struct BlockWorker {
     // to shared memory here).  The slot loops are unrolled by four and free of calls, so that
     // the loads of several slots are in flight together; the products are accumulated in
     // slot order in every variant.
+    // With the packed records (SysDev::ctaWord) a slot's column and phase index come in one
+    // word, and in FP32 with the coefficient in one 16-byte load.
     for (int r = threadIdx.x; r < D; r += blockDim.x) {
-      C2 acc = cmul(diag[r], ys[r]);
-      if (IP && tab) {
+      C2 acc = diagZero ? mk<C2>(0, 0) : cmul(diag[r], ys[r]);
+      if (IP && tab && word) {
+#pragma unroll 4
+        for (int s = 0; s < S; ++s) {
+          C2 c;
+          unsigned w;
+          slotRecord(s, r, c, w);
+          const unsigned k = w >> 16;
+          if (k != kNoPhase) {
+            const double2 ph = phTab[k];
+            c = mk<C2>(double(c.x) * ph.x - double(c.y) * ph.y, double(c.x) * ph.y + double(c.y) * ph.x);
+          }
+          acc = cfma(c, ys[r + int(short(w & 0xffffu))], acc);
+        }
+      } else if (IP && tab) {
 #pragma unroll 4
         for (int s = 0; s < S; ++s) {
           C2 c = __ldg(&val[s * D + r]);
@@ -139,11 +157,31 @@ struct BlockWorker {
           }
           acc = cfma(c, ys[__ldg(&col[s * D + r])], acc);
         }
+      } else if (word) {
+#pragma unroll 4
+        for (int s = 0; s < S; ++s) {
+          C2 c;
+          unsigned w;
+          slotRecord(s, r, c, w);
+          acc = cfma(c, ys[r + int(short(w & 0xffffu))], acc);
+        }
       } else {
 #pragma unroll 4
         for (int s = 0; s < S; ++s) acc = cfma(__ldg(&val[s * D + r]), ys[__ldg(&col[s * D + r])], acc);
       }
       out[r] = acc;
+    }
+  }
+
+  // coefficient and packed word of slot s of row r (SysDev::ctaWord / ctaRecF)
+  __device__ __forceinline__ void slotRecord(int s, int r, C2& c, unsigned& w) const {
+    if constexpr (sizeof(C2) == sizeof(float2)) {
+      const int4 q = __ldg(&recF[s * D + r]);
+      c = mk<C2>(__int_as_float(q.x), __int_as_float(q.y));
+      w = unsigned(q.z);
+    } else {
+      c = __ldg(&val[s * D + r]);
+      w = unsigned(__ldg(&word[s * D + r]));
     }
   }
 
@@ -577,6 +615,9 @@ __global__ void __launch_bounds__(512, 1) mcwfBlockKernel(TrajDev td, RunArgs ra
     w.col = s->col;
     w.val = Tables<R>::val(*s);
     w.diag = Tables<R>::diag(*s);
+    w.word = s->ctaWord;
+    w.recF = s->ctaRecF;
+    w.diagZero = s->diagZero != 0;
     w.freq = s->freq;
     // the phase table follows the broadcast words; shared-memory vectors follow the table
     double2* phTab = reinterpret_cast<double2*>(bcast + 8);

@@ -230,6 +230,13 @@ struct SysDev {
   const double2* wlambda;      // [Dp] (Exact) or null
   const unsigned short* wfIdx; // [kWarpSlots][Dp] (IP with a table) or null
   const double2* wfreq;        // [kWarpSlots][Dp] (IP) or null
+  // CTA-kernel records of the ELL tables (D < 32768; null otherwise): per slot and row one
+  // word, the column offset col - row as int16 in the low half and the distinct-frequency
+  // index (kNoPhase without one) in the high half; for FP32 the word rides in one 16-byte
+  // record with the coefficient {re, im, word, 0}, so a slot is one load
+  int diagZero;                // the fused main diagonal is all zero
+  const int* ctaWord;          // [S][D]
+  const int4* ctaRecF;         // [S][D]
   // precision-specific copies
   const double2* diagD;
   const double2* valD;
