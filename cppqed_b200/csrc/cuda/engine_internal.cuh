@@ -97,8 +97,8 @@ inline int defaultThreads(const KernelGroup& g) { return g.kind ? 256 : 128; }
 
 // Dynamic shared memory of the CTA kernel: two stage vectors of Dmax elements, the reduction
 // scratch and broadcast words, the interaction-picture phase table of phaseElems double2,
-// and with shared-memory vectors the kBlockVectors stage derivatives / candidate / cache of
-// ceil32(Dmax) elements each.
+// and with shared-memory vectors the kBlockVectors stage derivatives and second state buffer
+// of ceil32(Dmax) elements each.
 inline size_t blockSmemBytes(int Dmax, size_t elemBytes, bool vectors, int phaseElems) {
   const size_t base = 2 * size_t(Dmax) * elemBytes + 32 * (dev::MAX_JUMPS + 1) * sizeof(double) + 64 +
                       size_t(phaseElems) * sizeof(double2);

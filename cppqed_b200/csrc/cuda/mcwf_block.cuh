@@ -3,13 +3,17 @@
 // The warp kernel keeps a trajectory's state and stage derivatives in registers, which
 // limits it to D <= 128.  Here a CTA owns one trajectory at a time (persistent CTAs pull
 // trajectories from the same work queue) and each thread walks rows r = tid + blockDim*j.
-// The state stays in the trajectory's slot in device memory, the six Cash-Karp stage
-// derivatives, the candidate solution and the step-start cache live in a per-CTA scratch
-// slab (L2-resident for the CTAs in flight), and only the stage vector that the banded
-// H/i gather reads is staged in shared memory (double-buffered, one __syncthreads per
-// right-hand side).  Every row is touched by the same thread in every pass, so the
-// scratch vectors need no synchronisation.  The algorithm, step by step, is the one of
-// the warp kernel (mcwf_kernel.cuh) and of the reference's MCWF_Trajectory::step.
+// The state lives in two buffers, the trajectory's slot in device memory and one vector of a
+// per-CTA scratch slab: an ODE attempt writes its candidate solution into the buffer the
+// state is not in, an accepted attempt makes that buffer the state, and the other one still
+// holds the state of the step's start, which is all a step-back needs.  The stage
+// derivatives k0..k4 live in the scratch slab too (L2-resident for the CTAs in flight); k5
+// is consumed row by row by the solution and the error norm as the last right-hand side
+// produces it.  Only the stage vector that the banded H/i gather reads is staged in shared
+// memory (double-buffered, one __syncthreads per right-hand side).  Every row is touched by
+// the same thread in every pass, so the scratch vectors need no synchronisation.  The
+// algorithm, step by step, is the one of the warp kernel (mcwf_kernel.cuh) and of the
+// reference's MCWF_Trajectory::step.
 #pragma once
 
 #include "mcwf_kernel.cuh"
@@ -17,7 +21,7 @@
 namespace cqg {
 namespace dev {
 
-constexpr int kBlockVectors = 8;  // k0..k5, candidate solution, step-start cache
+constexpr int kBlockVectors = 6;  // k0..k4, the second state buffer
 
 // Cash-Karp stage tableau for the (not unrolled) stage loop
 __constant__ double kBlockA[5][5] = {{1. / 5, 0, 0, 0, 0},
@@ -40,14 +44,19 @@ __device__ __forceinline__ void blockSumN(double (&v)[N], int n, double* red) {
   warpSumN(v, n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   __syncthreads();
+  // loops over the compile-time bound, so that v stays in registers
   if (lane == 0)
-    for (int m = 0; m < n; ++m) red[warp * N + m] = v[m];
+#pragma unroll
+    for (int m = 0; m < N; ++m)
+      if (m < n) red[warp * N + m] = v[m];
   __syncthreads();
-  for (int m = 0; m < n; ++m) {
-    double s = 0.;
-    for (int w = 0; w < nw; ++w) s += red[w * N + m];
-    v[m] = s;
-  }
+#pragma unroll
+  for (int m = 0; m < N; ++m)
+    if (m < n) {
+      double s = 0.;
+      for (int w = 0; w < nw; ++w) s += red[w * N + m];
+      v[m] = s;
+    }
 }
 
 __device__ __forceinline__ double blockMax(double v, double* red) {
@@ -83,7 +92,9 @@ struct BlockWorker {
   const int* word;    // packed slot words (SysDev::ctaWord) or null
   const int4* recF;   // FP32 packed records (SysDev::ctaRecF) or null
   bool diagZero;      // the fused main diagonal is zero: not read
-  C2* x;       // the trajectory's state (device memory)
+  C2* x;       // the state: the trajectory's slot or the second buffer
+  C2* xalt;    // the other one (an attempt's candidate; after a step, the step's start)
+  C2* xslot;   // the trajectory's slot in device memory
   C2* vec;     // this CTA's scratch vectors
   long long stride;
   C2* ys0;     // shared stage buffers
@@ -98,11 +109,12 @@ struct BlockWorker {
   unsigned status;
 
   __device__ __forceinline__ C2* K(int j) const { return vec + j * stride; }
-  __device__ __forceinline__ C2* xnew() const { return vec + 6 * stride; }
-  __device__ __forceinline__ C2* cache() const { return vec + 7 * stride; }
+  __device__ __forceinline__ C2* second() const { return vec + 5 * stride; }
 
-  // out = (H/i) y at picture time tau, y in shared memory
-  __device__ __forceinline__ void rhs(const C2* ys, C2* out, double tau) {
+  // sink(r, ((H/i) y)[r]) for every row r of this thread, y in shared memory, at picture
+  // time tau
+  template <class Sink>
+  __device__ __forceinline__ void rhs(const C2* ys, double tau, Sink&& sink) {
     ++nRhs;
     bool tab = false;
     if constexpr (IP) {
@@ -111,7 +123,7 @@ struct BlockWorker {
       tab = phTab && hasFreq && tau != 0.;
       if (tab) {
         __syncthreads();
-        for (int k = threadIdx.x; k < nFD; k += blockDim.x) phTab[k] = cexpScaled(tau, __ldg(&fDist[k]));
+        for (int k = threadIdx.x; k < nFD; k += blockDim.x) phTab[k] = cexpScaledInline(tau, __ldg(&fDist[k]));
         __syncthreads();
       }
     }
@@ -169,7 +181,7 @@ struct BlockWorker {
 #pragma unroll 4
         for (int s = 0; s < S; ++s) acc = cfma(__ldg(&val[s * D + r]), ys[__ldg(&col[s * D + r])], acc);
       }
-      out[r] = acc;
+      sink(r, acc);
     }
   }
 
@@ -192,7 +204,10 @@ struct BlockWorker {
     __syncthreads();
     for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
     __syncthreads();
-    rhs(ys0, K(0), t - t0);
+    {
+      C2* const k0 = K(0);
+      rhs(ys0, t - t0, [&](int r, C2 v) { k0[r] = v; });
+    }
     for (int attempt = 0;; ++attempt) {
       if (attempt >= ra.maxAttempts) {
         status |= 8u;
@@ -213,19 +228,27 @@ struct BlockWorker {
           ys[r] = y;
         }
         __syncthreads();
-        rhs(ys, K(st), t + kBlockC[st - 1] * dt - t0);
+        if (st == 5) break;  // the last right-hand side feeds the solution below
+        C2* const ks = K(st);
+        rhs(ys, t + kBlockC[st - 1] * dt - t0, [&](int r, C2 v) { ks[r] = v; });
       }
       const R b0 = R(dt * CK::b0), b2 = R(dt * CK::b2), b3 = R(dt * CK::b3), b5 = R(dt * CK::b5);
       const R e0 = R(dt * CK::e0), e2 = R(dt * CK::e2), e3 = R(dt * CK::e3), e4 = R(dt * CK::e4),
               e5 = R(dt * CK::e5);
       const double adt = fabs(dt);
       ErrNormMax errLocal;
-      for (int r = threadIdx.x; r < D; r += blockDim.x) {
-        const C2 xr = x[r], k0 = K(0)[r], k2 = K(2)[r], k3 = K(3)[r], k4 = K(4)[r], k5 = K(5)[r];
-        xnew()[r] = axpy(b5, k5, axpy(b3, k3, axpy(b2, k2, axpy(b0, k0, xr))));
-        C2 xe = mk<C2>(0, 0);
-        xe = axpy(e5, k5, axpy(e4, k4, axpy(e3, k3, axpy(e2, k2, axpy(e0, k0, xe)))));
-        errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(xr) + adt * cabs(k0)));
+      // k5 row by row: the 5th-order solution into the other state buffer and the rows' part
+      // of the error norm
+      {
+        const C2* const xs = x;
+        C2* const cand = xalt;
+        rhs(ys1, t + kBlockC[4] * dt - t0, [&](int r, C2 k5) {
+          const C2 xr = xs[r], k0 = K(0)[r], k2 = K(2)[r], k3 = K(3)[r], k4 = K(4)[r];
+          cand[r] = axpy(b5, k5, axpy(b3, k3, axpy(b2, k2, axpy(b0, k0, xr))));
+          C2 xe = mk<C2>(0, 0);
+          xe = axpy(e5, k5, axpy(e4, k4, axpy(e3, k3, axpy(e2, k2, axpy(e0, k0, xe)))));
+          errLocal.add(abs2(xe), ra.absSlot + ra.relSlot * (cabs(xr) + adt * cabs(k0)));
+        });
       }
       const double err = blockMax(errLocal.value(), red);
       if (!(err == err)) {
@@ -243,7 +266,9 @@ struct BlockWorker {
       }
       t += dt;
       dtTry = err < 0.5 ? increasedStep(dt, err) : dt;
-      for (int r = threadIdx.x; r < D; r += blockDim.x) x[r] = xnew()[r];
+      C2* const start = x;  // the candidate becomes the state; the step's start stays behind
+      x = xalt;
+      xalt = start;
       break;
     }
     dtDid = t - timeBefore;
@@ -270,40 +295,57 @@ struct BlockWorker {
       const double stepToDo = li ? fmin(dtTry, Dt) : Dt;
       t += stepToDo;
       dtDid = stepToDo;
-    }
-    if (hasEx) {
-      const double tau = t - t0;
-      for (int r = threadIdx.x; r < D; r += blockDim.x) {
-        const double2 u = cexpScaled(tau, __ldg(&sysp->lambda[r]));
-        const C2 v = x[r];
-        x[r] = mk<C2>(double(v.x) * u.x - double(v.y) * u.y, double(v.x) * u.y + double(v.y) * u.x);
+      if (li) {  // the state is changed in place below: keep the step's start for a step-back
+        for (int r = threadIdx.x; r < D; r += blockDim.x) xalt[r] = x[r];
+        C2* const start = x;
+        x = xalt;
+        xalt = start;
       }
-      t0 = t;
     }
+    // One pass over the state: the exact part (Exact::actWithU), the state staged for the
+    // special jumps, the norm and the closed-form rates, each sum over this thread's rows in
+    // row order.
     double v[NR];
     for (int m = 0; m < NR; ++m) v[m] = 0.;
-    if (li && anySpecial) {
-      __syncthreads();
-      for (int r = threadIdx.x; r < D; r += blockDim.x) ys0[r] = x[r];
-      __syncthreads();
+    const bool stage = li && anySpecial;
+    if (stage) __syncthreads();
+    {
+      const double tau = t - t0;
+      unsigned wMask = 0u;  // jumps with closed-form rate weights
+      if (li)
+        for (int m = 0; m < nJ; ++m)
+          if (sysp->jHasW[m]) wMask |= 1u << m;
+      const double* const jw = sysp->jw;
+      for (int r = threadIdx.x; r < D; r += blockDim.x) {
+        C2 a = x[r];
+        if (hasEx) {
+          const double2 u = cexpScaledInline(tau, __ldg(&sysp->lambda[r]));
+          a = mk<C2>(double(a.x) * u.x - double(a.y) * u.y, double(a.x) * u.y + double(a.y) * u.x);
+          x[r] = a;
+        }
+        if (stage) ys0[r] = a;
+        const double a2 = abs2(a);
+        v[0] += a2;
+#pragma unroll
+        for (int m = 0; m < MAX_JUMPS; ++m)
+          if (wMask >> m & 1u) v[m + 1] += __ldg(&jw[size_t(m) * D + r]) * a2;
+      }
     }
-    for (int r = threadIdx.x; r < D; r += blockDim.x) v[0] += abs2(x[r]);
+    if (hasEx) t0 = t;
+    if (stage) __syncthreads();
     int nRed = 1;
     if (li) {
       for (int m = 0; m < nJ; ++m) {
+        if (sysp->jHasW[m]) continue;  // summed in the pass above
+        // special jump: rate |J_m psi|^2 from the staged state
         double acc = 0.;
-        if (sysp->jHasW[m]) {
-          const double* w = sysp->jw + size_t(m) * D;
-          for (int r = threadIdx.x; r < D; r += blockDim.x) acc += __ldg(&w[r]) * abs2(x[r]);
-        } else {
-          const int SJ = sysp->SJ;
-          const C2* jv = Tables<R>::jval(*sysp) + size_t(m) * SJ * D;
-          const int* jc = sysp->jcol + size_t(m) * SJ * D;
-          for (int r = threadIdx.x; r < D; r += blockDim.x) {
-            C2 a = mk<C2>(0, 0);
-            for (int s = 0; s < SJ; ++s) a = cfma(jv[s * D + r], ys0[jc[s * D + r]], a);
-            acc += abs2(a);
-          }
+        const int SJ = sysp->SJ;
+        const C2* jv = Tables<R>::jval(*sysp) + size_t(m) * SJ * D;
+        const int* jc = sysp->jcol + size_t(m) * SJ * D;
+        for (int r = threadIdx.x; r < D; r += blockDim.x) {
+          C2 a = mk<C2>(0, 0);
+          for (int s = 0; s < SJ; ++s) a = cfma(jv[s * D + r], ys0[jc[s * D + r]], a);
+          acc += abs2(a);
         }
 #pragma unroll
         for (int q = 0; q < MAX_JUMPS; ++q)
@@ -423,9 +465,8 @@ struct BlockWorker {
   __device__ __forceinline__ bool step(double Dt, const TrajDev& td) {
     const bool li = ra.noise && nJ > 0;
     const double tCache = t, dtDidCache = dtDid;
-    if (li)
-      for (int r = threadIdx.x; r < D; r += blockDim.x) cache()[r] = x[r];
     double rates[MAX_JUMPS];
+    // with jumps, coherentAndRates leaves the step's start untouched in xalt
     if (!coherentAndRates(Dt, li, rates)) return false;
     if (li) {
       int backs = 0;
@@ -434,7 +475,9 @@ struct BlockWorker {
           status |= 8u;
           return false;
         }
-        for (int r = threadIdx.x; r < D; r += blockDim.x) x[r] = cache()[r];
+        C2* const discarded = x;  // back to the step's start
+        x = xalt;
+        xalt = discarded;
         if (!coherentAndRates(Dt, li, rates)) return false;
       }
       if (!performJump(rates, td)) return false;
@@ -520,7 +563,9 @@ struct BlockWorker {
 
   __device__ __forceinline__ void run(const TrajDev& td, int trajIndex) {
     ti = (unsigned long long)trajIndex;
-    x = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
+    xslot = reinterpret_cast<C2*>(td.psi) + td.psiOff[trajIndex];
+    x = xslot;
+    xalt = second();
     t = td.t[ti];
     t0 = td.t0[ti];
     dtTry = td.dtTry[ti];
@@ -558,6 +603,8 @@ struct BlockWorker {
         if (threadIdx.x == 0) slot[ra.nAvrStride - 1] = dtDid;
       }
     }
+    if (x != xslot)  // the state ended in the second buffer (each thread copies its own rows)
+      for (int r = threadIdx.x; r < D; r += blockDim.x) xslot[r] = x[r];
     __syncthreads();
     if (threadIdx.x < 4) td.rng[4 * ti + threadIdx.x] = bcast[threadIdx.x];
     if (threadIdx.x == 0) {

@@ -97,14 +97,17 @@ template <typename C2>
 __device__ __forceinline__ double cabs(C2 a) {
   return sqrt(double(a.x) * double(a.x) + double(a.y) * double(a.y));
 }
-// exp(tau * f) for complex f, in double.  Kept out of line: sincos/exp expand to a lot
-// of code and are only needed in the interaction picture.
-static __device__ __noinline__ double2 cexpScaled(double tau, double2 f) {
+// exp(tau * f) for complex f, in double.  cexpScaled is kept out of line: sincos/exp expand
+// to a lot of code and are only needed in the interaction picture; the CTA kernel's per-row
+// loops take the inline form (same operations, same results), where a call would save and
+// restore the loop's live registers through local memory on every row.
+__device__ __forceinline__ double2 cexpScaledInline(double tau, double2 f) {
   double s, c;
   sincos(tau * f.y, &s, &c);
   const double m = exp(tau * f.x);
   return make_double2(m * c, m * s);
 }
+static __device__ __noinline__ double2 cexpScaled(double tau, double2 f) { return cexpScaledInline(tau, f); }
 
 // complex product with explicit roundings (no contraction choices left to the compiler)
 __device__ __forceinline__ double2 cmulD(double2 a, double2 b) {
