@@ -145,18 +145,43 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML read every 20 ms
+    (the device matched by PCI bus id), else nvidia-smi every 200 ms.  Read-only queries."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, set of reasons)
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.device)
+        bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.nvml = (nv, h, bits)
+            self.stopping = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -166,34 +191,50 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        nv, h, bits = self.nvml
+        while not self.stopping.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self.stopping.wait(0.02)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sms, maxes, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
-            p = [x.strip() for x in l.split(",")]
-            if len(p) < 9:
-                continue
+        if self.nvml is not None:
+            self.stopping.set()
+            self.thread.join(timeout=5)
+            source = "nvml, 20 ms"
+        elif self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        else:
+            self.proc.terminate()
             try:
-                sms.append(float(p[1]))
-                maxes.append(float(p[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            source = "nvidia-smi, 200 ms"
+            for l in self.lines:
+                p = [x.strip() for x in l.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    self.samples.append((float(p[1]), float(p[2]),
+                                         {n for n, v in zip(self.NAMES, p[5:9]) if v.lower() == "active"}))
+                except ValueError:
+                    continue
+        sms = [a for a, _, _ in self.samples]
+        maxes = [b for _, b, _ in self.samples]
+        reasons = set().union(*[c for _, _, c in self.samples]) if self.samples else set()
         return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": max(maxes) if maxes else None,
-                "reasons": sorted(reasons), "samples": len(sms)}
+                "reasons": sorted(reasons), "samples": len(sms), "source": source}
 
 
 def flops_model(model):

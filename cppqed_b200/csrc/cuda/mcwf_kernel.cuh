@@ -352,8 +352,13 @@ struct CK {
 };
 
 // Per-warp shared scratch next to the state slabs.
-struct WarpScratch {
+// The rarely changed logger counters and maxima live here rather than in registers; the
+// registers they free shorten the spills of the hot loops.  Lane 0 keeps them (every lane
+// holds the same warp-uniform values).
+struct alignas(16) WarpScratch {
   unsigned long long pcg[4];  // state hi, lo, increment hi, lo (pcg64); word 0 = draw count (philox)
+  double mx[3];               // maximal dpLimit overshoot, maximal tolerance overshoot, norm deviation
+  unsigned cnt[4];            // failed attempts, dpLimit overshoots, step-backs, jumps
 };
 
 // IP: the instance serves interaction-picture systems (rows with frequencies); Schroedinger-
@@ -401,9 +406,15 @@ struct Worker {
   double t, t0, dtTry, dtDid;
   unsigned long long ti;
   // per-launch counter increments
-  unsigned nSteps, nAttempts, nFailed, nRhs, nOvershot, nBacks, nJumps;
-  double maxOvershoot, maxTolOvershoot, maxNormDev;
+  unsigned nSteps, nAttempts, nRhs;
   unsigned status;
+  // rare logger counter c += 1, maximum c = max(maximum c, v) (WarpScratch::cnt / mx)
+  __device__ __forceinline__ void bump(int c) {
+    if (lane == 0) ws->cnt[c] += 1u;
+  }
+  __device__ __forceinline__ void maxTo(int c, double v) {
+    if (lane == 0) ws->mx[c] = fmax(ws->mx[c], v);
+  }
 
   __device__ __forceinline__ Worker(const SysDev* s, const RunArgs& a, int l, C2* b0, C2* b1, C2* c, WarpScratch* w,
                                     double2* ph)
@@ -669,7 +680,7 @@ struct Worker {
       }
       if (err > 1.0) {
         dtTry = decreasedStep(dt, err);
-        ++nFailed;
+        bump(0);
         if (!(dtTry > 0.) || t + dtTry == t) {
           status |= 4u;  // CQG_TRAJ_DT_UNDERFLOW
           return false;
@@ -761,7 +772,7 @@ struct Worker {
     const double inv = 1. / n;
 #pragma unroll
     for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(x[e].x) * inv, double(x[e].y) * inv);
-    maxNormDev = fmax(maxNormDev, fabs(1. - n));
+    maxTo(2, fabs(1. - n));
     if (li) {
       bool ok = true;
       const double inv2 = 1. / red[0];
@@ -786,15 +797,15 @@ struct Worker {
       if (m < nJ) totalRate += rates[m];
     const double liouvilleanSuggestedDtTry = ra.dpLimit / totalRate;
     if (totalRate * dtDid > ra.overTol * ra.dpLimit) {
-      maxTolOvershoot = fmax(maxTolOvershoot, totalRate * dtDid);
+      maxTo(1, totalRate * dtDid);
       t = tCache;
       dtDid = dtDidCache;
       dtTry = liouvilleanSuggestedDtTry;
-      ++nBacks;
+      bump(2);
       return true;
     } else if (totalRate * dtTry > ra.dpLimit) {
-      ++nOvershot;
-      maxOvershoot = fmax(maxOvershoot, totalRate * dtTry);
+      bump(1);
+      maxTo(0, totalRate * dtTry);
     }
     dtTry = hasH ? fmin(dtTry, liouvilleanSuggestedDtTry) : liouvilleanSuggestedDtTry;
     return false;
@@ -850,12 +861,12 @@ struct Worker {
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = mk<C2>(double(jx[e].x) * inv, double(jx[e].y) * inv);
       if (lane == 0 && td.jumpCap > 0) {
-        const unsigned long long total = __ldcg(&td.jumpN[ti]) + nJumps;
+        const unsigned long long total = __ldcg(&td.jumpN[ti]) + ws->cnt[3];
         const unsigned long long slot = total % (unsigned long long)td.jumpCap;
         td.jumpT[ti * td.jumpCap + slot] = t;
         td.jumpL[ti * td.jumpCap + slot] = lindbladNo;
       }
-      ++nJumps;
+      bump(3);
     }
     return true;
   }
@@ -937,10 +948,13 @@ struct Worker {
     dtDid = __ldcg(&td.dtDid[ti]);
     if (lane < 4) ws->pcg[lane] = __ldcg(&td.rng[4 * ti + lane]);
     __syncwarp();
-    nSteps = nAttempts = nFailed = nRhs = nOvershot = nBacks = nJumps = 0;
-    maxOvershoot = __ldcg(&td.maxima[3 * ti]);
-    maxTolOvershoot = __ldcg(&td.maxima[3 * ti + 1]);
-    maxNormDev = __ldcg(&td.maxima[3 * ti + 2]);
+    nSteps = nAttempts = nRhs = 0;
+    if (lane == 0) {
+      ws->cnt[0] = ws->cnt[1] = ws->cnt[2] = ws->cnt[3] = 0u;
+      ws->mx[0] = __ldcg(&td.maxima[3 * ti]);
+      ws->mx[1] = __ldcg(&td.maxima[3 * ti + 1]);
+      ws->mx[2] = __ldcg(&td.maxima[3 * ti + 2]);
+    }
     status = __ldcg(&td.status[ti]);
     ResumeInfo rs{0., 0, 0, 0};
     if (ra.resume) {
@@ -1010,17 +1024,17 @@ struct Worker {
       unsigned long long* cw = td.cnt + 8 * ti;
       cw[0] = __ldcg(&cw[0]) + nSteps;
       cw[1] = __ldcg(&cw[1]) + nAttempts;
-      cw[2] = __ldcg(&cw[2]) + nFailed;
+      cw[2] = __ldcg(&cw[2]) + ws->cnt[0];
       cw[3] = __ldcg(&cw[3]) + nRhs;
-      cw[4] = __ldcg(&cw[4]) + nOvershot;
-      cw[5] = __ldcg(&cw[5]) + nBacks;
-      cw[6] = __ldcg(&cw[6]) + nJumps;
+      cw[4] = __ldcg(&cw[4]) + ws->cnt[1];
+      cw[5] = __ldcg(&cw[5]) + ws->cnt[2];
+      cw[6] = __ldcg(&cw[6]) + ws->cnt[3];
       cw[7] = status;
-      td.maxima[3 * ti] = maxOvershoot;
-      td.maxima[3 * ti + 1] = maxTolOvershoot;
-      td.maxima[3 * ti + 2] = maxNormDev;
+      td.maxima[3 * ti] = ws->mx[0];
+      td.maxima[3 * ti + 1] = ws->mx[1];
+      td.maxima[3 * ti + 2] = ws->mx[2];
       td.status[ti] = status;
-      td.jumpN[ti] = __ldcg(&td.jumpN[ti]) + nJumps;
+      td.jumpN[ti] = __ldcg(&td.jumpN[ti]) + ws->cnt[3];
       if (yielded) ra.resume[ti] = rs;
     }
     __syncwarp();
