@@ -719,6 +719,71 @@ def test_cta_kernel_shared_memory_vectors_are_bit_identical(gpu):
     assert np.array_equal(runs[0][1], runs[1][1])
 
 
+# dpLimit step-backs (MCWF_Trajectory::manageTimeStep): no golden run contains one, so the
+# tolerance is lowered until they are frequent (overshoot tolerance 1.05, dpLimit 0.05, a first
+# step of 1 from the vacuum): the oracle takes 5-11 step-backs per trajectory over t in [0, 2].
+@pytest.mark.parametrize("kernel,cutoff,threads,shared", [("warp", 40, 0, 0), ("cta_global", 100, 128, 0),
+                                                          ("cta_shared", 100, 128, 1)])
+def test_step_backs_replay_oracle(gpu, oracle, kernel, cutoff, threads, shared):
+    args = list(C2_ARGS)
+    args[args.index("--cutoff") + 1] = str(cutoff)
+    model = gpu.Model("QbitMode_C++QED", args)
+    pars = model.run_pars().mcwf
+    pars.overshoot_tolerance = 1.05
+    pars.dp_limit = 0.05
+    pars.dt_init = 1.0
+    pars.cta_threads = threads
+    pars.cta_shared_vectors = shared
+    sysd = gpu.System(model.desc)
+    n = 6
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    assert ens.plan()[0]["kind"] == {"warp": 0, "cta_global": 1, "cta_shared": 2}[kernel]
+    ens.run(0.5, 4)
+    counters = ens.counters()
+    agree, backs = 0, 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.5, 4)
+        backs += int(ref["counters"][5])
+        jt, jl = ens.jumps(i, 4096)
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
+            # steps, attempts, failed attempts, overshoots, step-backs, jumps
+            for c in (0, 1, 2, 4, 5, 6):
+                assert counters[i, c] == ref["counters"][c], (i, c, counters[i], ref["counters"])
+    assert backs >= 2 * n  # the step-back path ran
+    assert agree >= n - 1
+
+
+def test_hamiltonian_free_cta_trajectories_replay_oracle(gpu, oracle):
+    """A system without an H/i part (a lossy mode in the interaction picture, unpumped, from a
+    Fock state: D = 150, the CTA kernel; every step is the exact part, the rates and a jump
+    test) replays the oracle's trajectories."""
+    model = gpu.Model("PumpedLossyMode_C++QED", ["--picture", "IP", "--deltaC", "-1", "--eta", "0", "--kappa", "1",
+                                                 "--cutoff", "150", "--minitFock", "30", "--no_quadratures"])
+    assert model.desc.contents.n_ham == 0
+    pars = model.run_pars().mcwf
+    sysd = gpu.System(model.desc)
+    n = 4
+    ens = gpu.Ensemble(sysd, model.initial_state(), n, pars)
+    assert ens.plan()[0]["kind"] in (1, 2)
+    ens.run(0.05, 4)
+    counters = ens.counters()
+    agree = 0
+    for i in range(n):
+        ref = oracle.trajectory(model, pars, pars.prng_stream + i, 0.05, 4)
+        jt, jl = ens.jumps(i, 4096)
+        assert len(ref["jump_t"]) > 0
+        if len(jt) == len(ref["jump_t"]) and np.allclose(jt, ref["jump_t"], rtol=1e-9) and \
+                np.array_equal(jl, ref["jump_l"]):
+            agree += 1
+            assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
+            for c in (0, 4, 5, 6):
+                assert counters[i, c] == ref["counters"][c], (i, c, counters[i], ref["counters"])
+    assert agree >= n - 1
+
+
 # ---- special jumps (rate = |J psi|^2) and finite temperature against the master equation ----
 
 def _ensemble_vs_master_z(gpu, oracle, model, n, Dt, K, linear_cols, master_substeps=1):
