@@ -284,7 +284,11 @@ def measured_peaks():
 # launch.  Apply kernel: 65,536 states of the same system (the full 1 M-state batch is larger
 # than a capture should be); reads are exactly psi + dpsi, part of the dpsi write is still
 # in L2 when the launch ends.
-MCWF_TRAFFIC = {"workload": "qbitmode_jc_2x40", "precision": "fp64", "bytes": 6.177024e6}
+# DRAM bytes (read + write) and L2-to-SM bytes per MCWF launch from one ncu capture of the
+# first timed launch of each workload (profiles/mcwf*Kernel_*.md), by (workload, precision)
+MCWF_TRAFFIC = {("qbitmode_jc_2x40", "fp64"): {"dram": 6.547456e6 + 0.141568e6, "l2_to_sm": 551.390528e6},
+                ("particle_cavity_2560", "fp32"): {"dram": 68.205568e6 + 429.584896e6, "l2_to_sm": 14.248422e9},
+                ("particle_cavity_2560", "fp64"): {"dram": 620.328704e6 + 2554.575e6, "l2_to_sm": 21.379149e9}}
 APPLY_TRAFFIC = {"n_states": 65536, "bytes": 167.799040e6 + 33.929728e6, "algorithmic_bytes": 48.0 * 65536 * 80}
 
 
@@ -436,8 +440,8 @@ def run_ours(args, rank, world, dev):
                                                           [round(1e3 * v / n_e2e, 3) for v in phases]))},
         "roofline": {"bound": "fp64" if args.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak,
-                     "traffic": MCWF_TRAFFIC["bytes"] if (args.workload, args.precision) == (
-                         MCWF_TRAFFIC["workload"], MCWF_TRAFFIC["precision"]) else None,
+                     "traffic": MCWF_TRAFFIC.get((args.workload, args.precision), {}).get("dram"),
+                     "traffic_l2_to_sm": MCWF_TRAFFIC.get((args.workload, args.precision), {}).get("l2_to_sm"),
                      "peak_source": "measured FMA probe (cqg_probe_fma_peaks) on this GPU",
                      "flops_per_attempt": per_attempt, "nnz_h": nnz},
         "n_traj": n_traj, "model": model, "apply": apply, "plan": ens.plan(),
