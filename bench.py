@@ -286,9 +286,9 @@ def measured_peaks():
 # in L2 when the launch ends.
 # DRAM bytes (read + write) and L2-to-SM bytes per MCWF launch from one ncu capture of the
 # first timed launch of each workload (profiles/mcwf*Kernel_*.md), by (workload, precision)
-MCWF_TRAFFIC = {("qbitmode_jc_2x40", "fp64"): {"dram": 6.547456e6 + 0.141568e6, "l2_to_sm": 551.390528e6},
-                ("particle_cavity_2560", "fp32"): {"dram": 68.205568e6 + 429.584896e6, "l2_to_sm": 14.248422e9},
-                ("particle_cavity_2560", "fp64"): {"dram": 620.328704e6 + 2554.575e6, "l2_to_sm": 21.379149e9}}
+MCWF_TRAFFIC = {("qbitmode_jc_2x40", "fp64"): {"dram": 6.54464e6 + 0.159232e6, "l2_to_sm": 530.862816e6},
+                ("particle_cavity_2560", "fp32"): {"dram": 72.08704e6 + 466.320128e6, "l2_to_sm": 14.272849e9},
+                ("particle_cavity_2560", "fp64"): {"dram": 619.755264e6 + 2555.67e6, "l2_to_sm": 21.374789e9}}
 APPLY_TRAFFIC = {"n_states": 65536, "bytes": 167.799040e6 + 33.929728e6, "algorithmic_bytes": 48.0 * 65536 * 80}
 
 

@@ -277,6 +277,17 @@ std::vector<float2> toF2(const std::vector<dcomp>& v) {
   return r;
 }
 
+// Twiddle factors of the position averages' radix-2 transform: tw[k] = exp(2 pi i k / N),
+// k < N / 2, with the same sincospi the transform's butterflies would call (the butterfly of
+// span len at position pos reads tw[pos N / len]: the argument 2 pos / len = 2 k / N exactly).
+__global__ void twiddleKernel(double2* tw, int N) {
+  for (int k = threadIdx.x; k < N / 2; k += blockDim.x) {
+    double s, c;
+    sincospi(double(2 * k) / double(N), &s, &c);
+    tw[k] = make_double2(c, s);
+  }
+}
+
 void buildSystemDevice(cqg_system& s) {
   const auto& L = s.L;
   const int64_t D = L.D;
@@ -371,6 +382,8 @@ void buildSystemDevice(cqg_system& s) {
       }
   }
   const size_t oCtaWord = A.add(ctaWord.size() * 4 + 16), oCtaRecF = A.add(ctaRecF.size() * 16 + 16);
+  const int nTw = L.fourierObs.empty() ? 0 : int(L.fourierN / 2);
+  const size_t oFTw = A.add(size_t(nTw) * 16 + 16);
   // The warp kernel's padded copies of the hot tables (see SysDev::wcol): rows to
   // Dp = 32 ceil(D / 32), slots to kWarpSlots, zero coefficients on the row itself.
   const bool warpTables = D <= kWarpKernelMaxD && S <= dev::kWarpSlots;
@@ -511,6 +524,14 @@ void buildSystemDevice(cqg_system& s) {
   sd.wlambda = wlambda.empty() ? nullptr : reinterpret_cast<const double2*>(b + oWlambda);
   sd.wfIdx = wfIdx.empty() ? nullptr : reinterpret_cast<const unsigned short*>(b + oWfIdx);
   sd.wfreq = wfreq.empty() ? nullptr : reinterpret_cast<const double2*>(b + oWfreq);
+  sd.fTw = nullptr;
+  if (nTw > 0) {
+    double2* tw = reinterpret_cast<double2*>(b + oFTw);
+    twiddleKernel<<<1, 256>>>(tw, int(L.fourierN));
+    ck(cudaGetLastError(), "twiddle kernel launch");
+    ck(cudaStreamSynchronize(0), "twiddle kernel");
+    sd.fTw = tw;
+  }
 }
 
 // ---- kernel dispatch -------------------------------------------------------------

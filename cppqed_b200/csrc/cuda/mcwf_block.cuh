@@ -505,8 +505,8 @@ struct BlockWorker {
           const int half = len >> 1;
           for (int bf = lane; bf < (N >> 1); bf += 32) {
             const int pos = bf % half, i0 = (bf / half) * len + pos, i1 = i0 + half;
-            double sw, cw;
-            sincospi(double(2 * pos) / double(len), &sw, &cw);  // exp(+2 pi i pos / len)
+            const double2 tw = __ldg(&sysp->fTw[pos * (N / len)]);  // exp(+2 pi i pos / len)
+            const double sw = tw.y, cw = tw.x;
             const C2 a = buf[i0], bb = buf[i1];
             const R tx = R(cw) * bb.x - R(sw) * bb.y, ty = R(cw) * bb.y + R(sw) * bb.x;
             buf[i0] = mk<C2>(double(a.x + tx), double(a.y + ty));
@@ -517,7 +517,9 @@ struct BlockWorker {
         for (int m = lane; m < N; m += 32) {
           const C2 yv = buf[(m + (N >> 1)) & (N - 1)];
           const double p = (double(yv.x) * double(yv.x) + double(yv.y) * double(yv.y)) / double(N);
-          for (int f = 0; f < nF; ++f) v[f] += __ldg(&sysp->fW[size_t(f) * N + m]) * p;
+#pragma unroll
+          for (int f = 0; f < 4; ++f)  // over the compile-time bound: v stays in registers
+            if (f < nF) v[f] += __ldg(&sysp->fW[size_t(f) * N + m]) * p;
         }
         __syncwarp();
       }

@@ -151,7 +151,12 @@ __device__ __forceinline__ void warpSumN(double (&v)[N], int n) {
 }
 
 // Odeint's default step adjuster (decrease: max(0.9 err^(-1/(error order - 1)), 0.2);
-// increase below err 0.5: 0.9 max(err, 5^-5)^(-1/stepper order)), out of line for code size.
+// increase below err 0.5: 0.9 max(err, 5^-5)^(-1/stepper order)).  The decrease (a double
+// pow, after a rejected attempt only) is out of line for code size.  The increase follows
+// nearly every accepted attempt and is a few instructions: inline, a call makes the caller
+// save and restore its live registers through local memory on every attempt (inline measured
+// +1 % on the FP64 warp kernel and +3-4 % on the CTA kernel; the FP32 warp kernel was no
+// faster inline and keeps the call).
 static __device__ __noinline__ double decreasedStep(double dt, double err) {
   return dt * fmax(0.9 * pow(err, -1. / 3.), 0.2);
 }
@@ -169,10 +174,11 @@ __device__ __forceinline__ double invFifthRoot(double err) {
   }
   return y;
 }
-static __device__ __noinline__ double increasedStep(double dt, double err) {
+__device__ __forceinline__ double increasedStep(double dt, double err) {
   err = fmax(3.2e-4, err);  // 5^-5
   return dt * 0.9 * invFifthRoot(err);
 }
+static __device__ __noinline__ double increasedStepCall(double dt, double err) { return increasedStep(dt, err); }
 
 // Running maximum over rows of |e_n| / den_n (the Odeint error norm) with no square root
 // or division per row: a row replaces the current maximum when |e|^2 den_max^2 >
@@ -214,6 +220,7 @@ struct SysDev {
   int fObs[4];           // their observable indices
   const int* oFourier;   // [nObs] 1: evaluated by the transform (CTA kernel), else 0
   const double* fW;      // [nF][fN] weights
+  const double2* fTw;    // [fN / 2] twiddle factors exp(2 pi i k / fN) of the transform
   const double2* freq;   // [S][D] (IP) or null
   int nFD;               // IP with a table: distinct nonzero values of freq
   const unsigned short* fIdx;  // [S][D] index of freq into fDist (kNoPhase: zero), or null
@@ -689,7 +696,14 @@ struct Worker {
         continue;
       }
       t += dt;
-      dtTry = err < 0.5 ? increasedStep(dt, err) : dt;
+      if (err < 0.5) {
+        if constexpr (sizeof(R) == sizeof(double))
+          dtTry = increasedStep(dt, err);
+        else
+          dtTry = increasedStepCall(dt, err);
+      } else {
+        dtTry = dt;
+      }
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = y[e];
       break;
@@ -725,11 +739,30 @@ struct Worker {
       dtDid = stepToDo;
     }
     if (hasEx) {
+      // Exact::actWithU.  FP64 states: the factors exp(tau lambda) of this lane's rows are
+      // formed by one inline copy of the exponential in a rolled loop and parked in the warp's
+      // first stage buffer (free between steps), then applied; an out-of-line call here, even
+      // never taken (Schroedinger-picture systems have no exact part), made the whole FP64
+      // kernel's register allocation worse (qubit-mode 2x40 FP64: +1.2 % without it).  The
+      // FP32 kernel measured 3 % slower that way and keeps one call per row.
       const double tau = t - t0;
+      if constexpr (sizeof(R) == sizeof(double)) {
+        double2* const u = reinterpret_cast<double2*>(buf0);
+        __syncwarp();  // every lane is done with the last stage's gathers
+#pragma unroll 1
+        for (int e = 0; e < E; ++e) u[row(e)] = cexpScaledInline(tau, __ldg(&sysp->wlambda[row(e)]));
 #pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const double2 u = cexpScaled(tau, __ldg(&sysp->wlambda[row(e)]));
-        x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
+        for (int e = 0; e < E; ++e) {
+          const double2 ue = u[row(e)];
+          x[e] = mk<C2>(double(x[e].x) * ue.x - double(x[e].y) * ue.y, double(x[e].x) * ue.y + double(x[e].y) * ue.x);
+        }
+        __syncwarp();
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const double2 u = cexpScaled(tau, __ldg(&sysp->wlambda[row(e)]));
+          x[e] = mk<C2>(double(x[e].x) * u.x - double(x[e].y) * u.y, double(x[e].x) * u.y + double(x[e].y) * u.x);
+        }
       }
       t0 = t;
     }

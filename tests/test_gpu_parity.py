@@ -779,7 +779,10 @@ def test_hamiltonian_free_cta_trajectories_replay_oracle(gpu, oracle):
                 np.array_equal(jl, ref["jump_l"]):
             agree += 1
             assert np.linalg.norm(ens.state(i, model.dim) - ref["psi"]) < 1e-7
-            for c in (0, 4, 5, 6):
+            # steps, step-backs, jumps.  Not the dpLimit overshoots: between jumps the state is a
+            # Fock state, its rate does not change, and rate x (dpLimit / rate) > dpLimit is a
+            # last-bit tie of the rate's summation order at every step.
+            for c in (0, 5, 6):
                 assert counters[i, c] == ref["counters"][c], (i, c, counters[i], ref["counters"])
     assert agree >= n - 1
 
