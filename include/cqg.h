@@ -166,7 +166,9 @@ typedef struct cqg_mcwf_pars {
                                   queue after this many MCWF steps and takes the next, so the
                                   end of a launch waits for one such chunk, not for whole
                                   trajectories; the results are bit-identical.  0: the default
-                                  (64), -1: never */
+                                  (64 for groups of Schroedinger-picture systems; groups with
+                                  interaction-picture phases do not yield), > 0: every warp
+                                  group, -1: never */
 } cqg_mcwf_pars;
 
 void cqg_mcwf_pars_default(cqg_mcwf_pars* p);
