@@ -1131,6 +1131,9 @@ __global__ void __launch_bounds__(128, MINB) mcwfWarpKernel(TrajDev td, RunArgs 
         const unsigned long long tw = globalTimerNs();
         volatile int* seq = ra.yieldSeq;
         volatile int* done = ra.doneCount;
+        // the polls back off (128 ns doubling to 4 us): the waiting warps of a launch's tail
+        // would otherwise keep the queue's few cache lines busy for the warps that still run
+        unsigned sleepNs = 128;
         while (true) {
           if (seq[p] == p + 1) {
             __threadfence();
@@ -1142,7 +1145,8 @@ __global__ void __launch_bounds__(128, MINB) mcwfWarpKernel(TrajDev td, RunArgs 
             atomicOr(ra.queueError, 1u);
             break;
           }
-          __nanosleep(256);
+          __nanosleep(sleepNs);
+          if (sleepNs < 4096) sleepNs <<= 1;
         }
       }
       got = __shfl_sync(FULL, got, 0);
