@@ -153,10 +153,8 @@ __device__ __forceinline__ void warpSumN(double (&v)[N], int n) {
 // Odeint's default step adjuster (decrease: max(0.9 err^(-1/(error order - 1)), 0.2);
 // increase below err 0.5: 0.9 max(err, 5^-5)^(-1/stepper order)).  The decrease (a double
 // pow, after a rejected attempt only) is out of line for code size.  The increase follows
-// nearly every accepted attempt and is a few instructions: inline, a call makes the caller
-// save and restore its live registers through local memory on every attempt (inline measured
-// +1 % on the FP64 warp kernel and +3-4 % on the CTA kernel; the FP32 warp kernel was no
-// faster inline and keeps the call).
+// nearly every accepted attempt and is a few instructions: inline, since a call makes the
+// caller save and restore its live registers through local memory on every attempt.
 static __device__ __noinline__ double decreasedStep(double dt, double err) {
   return dt * fmax(0.9 * pow(err, -1. / 3.), 0.2);
 }
@@ -178,7 +176,6 @@ __device__ __forceinline__ double increasedStep(double dt, double err) {
   err = fmax(3.2e-4, err);  // 5^-5
   return dt * 0.9 * invFifthRoot(err);
 }
-static __device__ __noinline__ double increasedStepCall(double dt, double err) { return increasedStep(dt, err); }
 
 // Running maximum over rows of |e_n| / den_n (the Odeint error norm) with no square root
 // or division per row: a row replaces the current maximum when |e|^2 den_max^2 >
@@ -696,14 +693,7 @@ struct Worker {
         continue;
       }
       t += dt;
-      if (err < 0.5) {
-        if constexpr (sizeof(R) == sizeof(double))
-          dtTry = increasedStep(dt, err);
-        else
-          dtTry = increasedStepCall(dt, err);
-      } else {
-        dtTry = dt;
-      }
+      dtTry = err < 0.5 ? increasedStep(dt, err) : dt;
 #pragma unroll
       for (int e = 0; e < E; ++e) x[e] = y[e];
       break;
